@@ -1,0 +1,139 @@
+/* r3d_gpu.h - C ABI of the B200 Rast-3DMHD time step (librast3d_b200.so).
+ *
+ * The reference binds its GPU step through C++ entry points in include/gpu.hpp:18-49
+ * (gpu_alloc / gpu_upload / step_gpu / gpu_download / gpu_free) and its configuration through
+ * include/params.hpp:24-158 (Params, Derived, parse_args).  This header is the same surface as
+ * plain C: plain structs, pointers and sizes, status codes instead of exit(), so that any host
+ * language can bind it.  Each entry point names the reference interface it replaces.
+ *
+ * Domain: one GPU holds the whole global domain that the reference splits over npey x npez MPI
+ * ranks.  Host arrays exchanged through this ABI use the reference layout on the global domain:
+ * (npx+2) x (npy+2) x (npz+2) doubles, x fastest, idx = i + NX*(j + NY*k), interior
+ * i in [1,npx], j in [1,npy], k in [1,npz]; ghost cells at the ends of every axis.
+ *
+ * Errors: every call returns R3D_OK (0) or a negative R3D_E* code; r3d_last_error() returns a
+ * message for the calling thread's most recent failure.  Nothing here calls exit().
+ */
+#ifndef R3D_GPU_H
+#define R3D_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    R3D_OK = 0,
+    R3D_EINVAL = -1,      /* bad argument / unsupported configuration */
+    R3D_ECUDA = -2,       /* CUDA runtime error */
+    R3D_ENOMEM = -3,      /* device or host allocation failed */
+    R3D_ESTATE = -4,      /* call out of order (e.g. step before upload) */
+    R3D_ENUMERIC = -5     /* non-finite dt or dt underflow detected by the step */
+};
+
+enum { R3D_PREC_FP64 = 0, R3D_PREC_FP32BULK = 1 };
+
+/* Run configuration: every field of the reference Params (include/params.hpp:24-120) with the
+ * same meaning and defaults, plus three extensions (seed, precision, stages_per_graph). */
+typedef struct r3d_params {
+    int npx, npy, npz, npey, ix, iy, ilap, ipad, ngrid, id, ncol, nrow;
+    int ixcon, iycon, izcon, itcon, ibcon;
+    int lrot, lmag, lpot, lrem, lshr;
+    int ncase, ncasep, ntotal, nstep0, nstart, ntube;
+    double re, pr, theta, grav, r_y, ang, rm, beta, pzp, sigma, polys, tp, tc, xp, yp, zp;
+    double xmax, ymax, zmax, ampt, ampb, bfh, bzp, qfh, gamma, hh, dh, dv, tstart, toff, rlax;
+    double xx1, xx2, yy1, yy2, zz1, zz2, xa, xb, xc, xd, ya, yb, yc, yd, za, zb, zc, zd;
+    double xcent, zcent, rmax, cmt, a_tube, lambda, vz0, sf;
+    int backend; /* 0 = cpu, 1 = gpu (reference --backend) */
+    int gpu_id;  /* reference --gpu */
+    /* extensions */
+    int seed;      /* --seed N: RAN2 seed idum = -N (reference hard-wires N = 62659) */
+    int precision; /* --precision fp64|fp32bulk */
+} r3d_params;
+
+/* Scalars the reference carries in SimState (include/fields.hpp:137-143). */
+typedef struct r3d_scalars {
+    double dt, timc, timt, timi, umach, tb;
+    int nit;
+} r3d_scalars;
+
+/* Host view of the state on the global domain (see layout above).  3D arrays hold
+ * NX*NY*NZ doubles; x/y/z lines hold NX/NY/NZ doubles.  bx/by/bz may be NULL when lmag = 0.
+ * Mirrors the reference SimState primaries + 1D metrics (include/fields.hpp:75-145). */
+typedef struct r3d_host_state {
+    double *ru, *rv, *rw, *ro, *tt, *bx, *by, *bz;
+    double *exx, *dxxdx, *d2xxdx2, *ddx;
+    double *wyy, *dyydy, *d2yydy2, *ddy;
+    double *zee, *dzzdz, *d2zzdz2, *ddz, *rkapa, *dkapa;
+} r3d_host_state;
+
+/* Per-kernel timing of r3d_gpu_run_timed (CUDA events on the library's stream). */
+typedef struct r3d_timing {
+    double total_ms;        /* whole run, first launch to last */
+    double stage_ms;        /* sum over the fused stage kernels */
+    double bcon_ms;         /* sum over BCON + ghost + dt-edge kernels */
+    double other_ms;        /* dt finalise / scalar kernels */
+    int stage_launches;
+    int total_launches;     /* kernels launched by the library in the run */
+} r3d_timing;
+
+typedef struct r3d_gpu r3d_gpu;
+
+/* ---- configuration (replaces Params defaults, parse_args, derive: src/params.cpp:14-266) ---- */
+int r3d_params_default(r3d_params* p);
+/* Parses reference flags ("--npx 32", "--lmag=1", ...) plus --seed and --precision on top of
+ * *p.  Unknown flags are an error (R3D_EINVAL), as in the reference.  argv excludes argv[0]. */
+int r3d_params_parse(int argc, const char* const* argv, r3d_params* p);
+/* Validates p for this implementation (stencil widths 2, periodic x/y, supported toggles). */
+int r3d_params_check(const r3d_params* p);
+/* Derived constants by name ("c13", "hx", "repr", ...); mirrors Derived (include/params.hpp:125-145). */
+int r3d_derived_get(const r3d_params* p, const char* name, double* out);
+/* Global grid sizes NX, NY, NZ. */
+int r3d_dims(const r3d_params* p, int64_t* nx, int64_t* ny, int64_t* nz);
+
+/* ---- host set-up: grid metrics + conductivity + static IC + ghost fill (src/main.cpp:134-154,
+ *      src/grid.cpp:148-284, src/static_ic.cpp:24-161, src/ode.cpp:152-174) ---------------- */
+int r3d_setup_host(const r3d_params* p, r3d_host_state* st, r3d_scalars* sc);
+/* Static polytrope T(k), R(k), k = 0..npz-1 (src/ode.cpp:152-174). */
+int r3d_static_profile(const r3d_params* p, double* t, double* r);
+
+/* ---- device state (replaces gpu_alloc / gpu_upload / gpu_download / gpu_free,
+ *      include/gpu.hpp:35-38) ----------------------------------------------------------- */
+int r3d_gpu_create(const r3d_params* p, r3d_gpu** out);
+int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc);
+int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc);
+int r3d_gpu_destroy(r3d_gpu* g);
+/* Bytes of device memory held by g. */
+int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes);
+/* The CUDA stream (cudaStream_t) every kernel of g is launched on. */
+void* r3d_gpu_stream(r3d_gpu* g);
+
+/* ---- time step (replaces step_gpu(comm, p, d, t, g, scalars) and step_gpu(nstages, ...),
+ *      include/gpu.hpp:43-49; semantics of step(), src/step.cpp:114-257) ------------------ */
+/* One RK3 step (nstages = 3) or its first nstages substages; updates *sc like the reference
+ * (dt, umach, nit, timc, timt).  Synchronises with the device to return the scalars. */
+int r3d_gpu_step(r3d_gpu* g, int nstages, r3d_scalars* sc);
+/* nsteps full steps queued back to back with no host synchronisation in between (unless the
+ * plume relaxation tc != 0 needs the host clock); then synchronises and returns scalars. */
+int r3d_gpu_run(r3d_gpu* g, int nsteps, r3d_scalars* sc);
+/* As r3d_gpu_run without the final synchronisation (sc may be NULL; scalars stay on device). */
+int r3d_gpu_enqueue(r3d_gpu* g, int nsteps);
+/* As r3d_gpu_run, recording CUDA events around every kernel launch into *tm. */
+int r3d_gpu_run_timed(r3d_gpu* g, int nsteps, r3d_scalars* sc, r3d_timing* tm);
+
+/* ---- FP32-bulk extras ---- */
+/* Volume sums of rho and of the total energy proxy over the interior, accumulated in FP64 on
+ * the device (mass = sum rho, energy = sum (rho*T*cv + 0.5*(ru^2+rv^2+rw^2)/rho)). */
+int r3d_gpu_totals(r3d_gpu* g, double* mass, double* energy);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* r3d_last_error(void);
+/* Library version string. */
+const char* r3d_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

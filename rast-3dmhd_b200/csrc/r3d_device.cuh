@@ -1,0 +1,86 @@
+// r3d_device.cuh - device-side data shared by the step kernels.
+//
+// Layout in HBM: one array per field over the global domain with one ghost layer per side,
+// element (i,j,k) at k*plane + j*pitch + i, i in [0, npx+1], j in [0, npy+1], k in [0, npz+1].
+// The row pitch is padded to a multiple of 16 doubles (128 B) so every row starts on a
+// 128-byte boundary; tiles that start at i = 32*t (the halo column of interior column 32*t+1)
+// are aligned for coalesced and TMA access.
+#pragma once
+
+#include <cstdint>
+
+namespace r3dk {
+
+constexpr int kMaxFields = 8;  // ru rv rw ro tt bx by bz
+
+// Everything a stage kernel needs besides the field pointers.  Host-computed products keep
+// the reference association (e.g. tmpy[j] = hy*dyydy[j], src/fluxes.cpp:90).
+struct Geometry {
+    int npx, npy, npz;
+    int64_t pitch;  // doubles per row
+    int64_t plane;  // doubles per z plane
+};
+
+struct Physics {
+    double hx, h2x, hy, hz;
+    double c13, c23, c43, ore, ocv, grav;
+    double tdiff;    // ocv/repr                     (src/fluxes.cpp:247)
+    double theat;    // ocv*ore                      (src/fluxes.cpp:344)
+    double theat43;  // c43*ocv*ore                  (src/fluxes.cpp:399)
+    double t13;      // c13*ore                      (src/fluxes.cpp:362)
+    double omx, omz;
+    double gamma, ogamma, re, repr, cv, rm, obeta, orm, sff;
+    double gam[3], zeta[3];
+    int lrot, lmag;
+    int kappa_const;  // rkapa == 1 and dkapa == 0 on every plane (exact shortcut)
+};
+
+// 1D metric tables (device pointers).
+struct Lines {
+    const double *dxxdx, *d2xxdx2, *ddx;                      // [npx+2]
+    const double *dyydy, *tmpy, *tmpy1, *tmpy2, *ddy;         // [npy+2]
+    const double *dzzdz, *d2zzdz2, *tmpz, *tmpz1, *tmpz2;     // [npz+2]
+    const double *ddz, *rkapa, *dkapa;                        // [npz+2]
+    const double *plume_x, *plume_y;                          // [npx+2], [npy+2]
+};
+
+// Boundary set-up for the BCON kernel (src/bcon.cpp:12-141).
+struct Boundary {
+    int top_mode;     // 0 const T=1, 1 const flux, 2 plume T, 3 plume flux, 4 half-domain T
+    int bottom_mode;  // 0 const T=tb, 1 const flux
+    double tpr, hh, theta, tp, dz_top, dz_bot, tb;
+    int half_nx;      // NX/2 for ITCON 4
+};
+
+// Device-resident scalars and the running dt reduction (ordered-integer keys).
+struct Scalars {
+    double dt, timc, timt, timi, umach, tb;
+    int nit;
+    int pad;
+    unsigned long long wmin[4];  // keys of min(ww1), min(ww2), min(ww3), min(vv)
+    unsigned long long umax;     // key of max(ogamma*uu/tt)
+    double mass, energy;         // diagnostics (r3d_gpu_totals)
+};
+
+// Total order on doubles as unsigned keys: key(a) < key(b) iff a < b (NaN excluded).
+__host__ __device__ inline unsigned long long order_key(double x) {
+    unsigned long long b;
+#ifdef __CUDA_ARCH__
+    b = (unsigned long long)__double_as_longlong(x);
+#else
+    __builtin_memcpy(&b, &x, 8);
+#endif
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__host__ __device__ inline double order_value(unsigned long long k) {
+    unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)b);
+#else
+    double x;
+    __builtin_memcpy(&x, &b, 8);
+    return x;
+#endif
+}
+
+}  // namespace r3dk

@@ -1,0 +1,493 @@
+// r3d_gpu.cu - the C ABI behind include/r3d_gpu.h: device state, upload/download and the
+// step sequence.
+//
+// Replaces GpuSim / gpu_alloc / gpu_upload / gpu_download / gpu_free / step_gpu
+// (src/gpu.cpp:185-384, 736-1052).  Differences by design:
+//  * the whole global domain lives on one device; the reference's y/z halo exchange becomes
+//    the ghost images that the stage and BCON kernels write (no MPI, no NCCL, no staging);
+//  * the state is double-buffered (X_a -> X_b) plus one accumulator Z per field, 15 arrays for
+//    hydro instead of the reference's 28 (F, UU.., WW1..3 and the rho snapshot are never
+//    stored);
+//  * dt, umach, nit, timc, timt live on the device; a step is 8 kernel launches with no host
+//    round trip (the reference copies three full arrays to the host per step for dt,
+//    src/gpu.cpp:790-823).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "r3d_device.cuh"
+#include "r3d_error.hpp"
+#include "r3d_gpu.h"
+#include "r3d_host.hpp"
+#include "r3d_kernels.h"
+
+using namespace r3db;
+using r3dk::FieldSet;
+
+namespace {
+
+inline void cuda_ok(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw Error(e == cudaErrorMemoryAllocation ? R3D_ENOMEM : R3D_ECUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+__global__ void totals_kernel(r3dk::Geometry g, r3dk::Physics ph, FieldSet fs, r3dk::Scalars* sc) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    double m = 0.0, e = 0.0;
+    if (i <= g.npx && j <= g.npy) {
+        for (int k = 1 + blockIdx.z; k <= g.npz; k += gridDim.z) {
+            const int64_t n = (int64_t)k * g.plane + (int64_t)j * g.pitch + i;
+            const double ru = fs.xin[0][n], rv = fs.xin[1][n], rw = fs.xin[2][n];
+            const double ro = fs.xin[3][n], tt = fs.xin[4][n];
+            m += ro;
+            e += ro * tt * ph.cv + 0.5 * (ru * ru + rv * rv + rw * rw) / ro;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        m += __shfl_xor_sync(0xffffffffu, m, o);
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&sc->mass, m);
+        atomicAdd(&sc->energy, e);
+    }
+}
+
+}  // namespace
+
+namespace r3dk {
+cudaError_t launch_totals(const Geometry& g, const Physics& ph, const FieldSet& fs, Scalars* sc,
+                          cudaStream_t st) {
+    dim3 block(32, 8, 1);
+    dim3 grid((g.npx + 31) / 32, (g.npy + 7) / 8, (unsigned)std::min(g.npz, 64));
+    totals_kernel<<<grid, block, 0, st>>>(g, ph, fs, sc);
+    return cudaGetLastError();
+}
+}  // namespace r3dk
+
+struct r3d_gpu {
+    r3d_params p;
+    Derived d;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    r3dk::Geometry geo{};
+    r3dk::Physics ph{};
+    r3dk::Lines lines{};
+    r3dk::Boundary bnd{};
+    int nfields = 5;
+    double* X[2][r3dk::kMaxFields] = {};
+    double* Z[r3dk::kMaxFields] = {};
+    double* line_buf = nullptr;
+    r3dk::Scalars* dsc = nullptr;
+    r3dk::Scalars* hsc = nullptr;  // pinned mirror
+    int cur = 0;
+    int kchunk = 32;
+    bool uploaded = false;
+    int64_t bytes = 0;
+    double host_timc = 0.0, host_timi = 0.0;  // host clock for the plume relaxation (tc != 0)
+    std::vector<cudaEvent_t> ev;             // timing events (r3d_gpu_run_timed)
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
+};
+
+FieldSet fieldset(const r3d_gpu* g) {
+    FieldSet fs{};
+    for (int q = 0; q < r3dk::kMaxFields; ++q) {
+        fs.xin[q] = g->X[g->cur][q];
+        fs.xout[q] = g->X[1 - g->cur][q];
+        fs.z[q] = g->Z[q];
+    }
+    return fs;
+}
+
+double plume_tpr(const r3d_gpu* g) {
+    const double timt = g->host_timc + g->host_timi;  // src/bcon.cpp:22
+    return (g->p.tc != 0.0) ? g->p.tp + (1.0 - g->p.tp) * std::exp(-timt / g->p.tc) : g->p.tp;
+}
+
+struct Timer {
+    r3d_gpu* g;
+    bool on;
+    r3d_timing* tm;
+    std::vector<std::pair<int, int>> spans;  // (event index, category)
+    int next = 0;
+    cudaEvent_t at(int idx) {
+        while ((int)g->ev.size() <= idx) {
+            cudaEvent_t e;
+            cuda_ok(cudaEventCreate(&e), "cudaEventCreate");
+            g->ev.push_back(e);
+        }
+        return g->ev[idx];
+    }
+    void begin() {
+        if (on) cuda_ok(cudaEventRecord(at(next), g->stream), "cudaEventRecord");
+    }
+    void end(int cat) {
+        if (!on) return;
+        cuda_ok(cudaEventRecord(at(next + 1), g->stream), "cudaEventRecord");
+        spans.push_back({next, cat});
+        next += 2;
+    }
+};
+
+// Queue one step (nstages substages) on the device.
+void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_launches) {
+    g->bnd.tpr = plume_tpr(g);
+    tm.begin();
+    cuda_ok(r3dk::launch_step_begin(g->ph, g->dsc, g->stream), "step_begin");
+    tm.end(2);
+    ++launches;
+    for (int s = 0; s < nstages; ++s) {
+        FieldSet fs = fieldset(g);
+        tm.begin();
+        if (g->p.lmag)
+            cuda_ok(r3dk::launch_stage_mhd_fp64(s, g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage_mhd");
+        else
+            cuda_ok(r3dk::launch_stage_fp64(s, g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage");
+        tm.end(0);
+        tm.begin();
+        cuda_ok(r3dk::launch_bcon(g->geo, g->ph, g->lines, g->bnd, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon");
+        tm.end(1);
+        launches += 2;
+        ++stage_launches;
+        g->cur = 1 - g->cur;
+    }
+    tm.begin();
+    cuda_ok(r3dk::launch_step_end(g->dsc, g->stream), "step_end");
+    ++launches;
+    if (nstages < 3) {  // the next dt needs the limits of this (partial-step) state
+        FieldSet fs = fieldset(g);
+        cuda_ok(r3dk::launch_dt_full(g->geo, g->ph, g->lines, fs, g->dsc, g->stream), "dt_full");
+        ++launches;
+    }
+    tm.end(2);
+}
+
+void pull_scalars(r3d_gpu* g, r3d_scalars* sc) {
+    cuda_ok(cudaMemcpyAsync(g->hsc, g->dsc, sizeof(r3dk::Scalars), cudaMemcpyDeviceToHost, g->stream),
+            "scalar read-back");
+    cuda_ok(cudaStreamSynchronize(g->stream), "step");
+    g->host_timc = g->hsc->timc;
+    g->host_timi = g->hsc->timi;
+    if (sc) {
+        sc->dt = g->hsc->dt;
+        sc->timc = g->hsc->timc;
+        sc->timt = g->hsc->timt;
+        sc->timi = g->hsc->timi;
+        sc->umach = g->hsc->umach;
+        sc->tb = g->hsc->tb;
+        sc->nit = g->hsc->nit;
+    }
+}
+
+void run_steps(r3d_gpu* g, int nsteps, r3d_scalars* sc, r3d_timing* tmout, bool sync) {
+    if (!g) throw std::invalid_argument("null handle");
+    if (!g->uploaded) throw Error(R3D_ESTATE, "step before upload");
+    if (nsteps < 0) throw std::invalid_argument("nsteps < 0");
+    DeviceGuard dg(g->device);
+    Timer tm{g, tmout != nullptr, tmout};
+    int launches = 0, stage_launches = 0;
+    for (int n = 0; n < nsteps; ++n) {
+        enqueue_step(g, 3, tm, launches, stage_launches);
+        if (g->p.tc != 0.0 && n + 1 < nsteps) pull_scalars(g, nullptr);  // host clock for BCON
+    }
+    if (sync || tmout) pull_scalars(g, sc);
+    if (tmout) {
+        std::memset(tmout, 0, sizeof(*tmout));
+        for (auto& sp : tm.spans) {
+            float ms = 0.f;
+            cuda_ok(cudaEventElapsedTime(&ms, g->ev[sp.first], g->ev[sp.first + 1]), "event time");
+            if (sp.second == 0) tmout->stage_ms += ms;
+            else if (sp.second == 1) tmout->bcon_ms += ms;
+            else tmout->other_ms += ms;
+        }
+        if (!tm.spans.empty()) {
+            float ms = 0.f;
+            cuda_ok(cudaEventElapsedTime(&ms, g->ev[tm.spans.front().first], g->ev[tm.spans.back().first + 1]),
+                    "event time");
+            tmout->total_ms = ms;
+        }
+        tmout->stage_launches = stage_launches;
+        tmout->total_launches = launches;
+    }
+}
+
+void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
+    const r3d_params& p = g->p;
+    const Derived& d = g->d;
+    const int64_t NX = d.nx, NY = d.ny, NZ = d.nz;
+    // host tables (products keep the reference association)
+    std::vector<double> dxxdx(st->dxxdx, st->dxxdx + NX), d2xxdx2(st->d2xxdx2, st->d2xxdx2 + NX),
+        ddx(st->ddx, st->ddx + NX);
+    std::vector<double> dyydy(st->dyydy, st->dyydy + NY), ddy(st->ddy, st->ddy + NY);
+    std::vector<double> tmpy(NY), tmpy1(NY), tmpy2(NY);
+    for (int64_t j = 0; j < NY; ++j) {
+        tmpy[j] = d.hy * st->dyydy[j];                       // src/fluxes.cpp:90
+        tmpy1[j] = d.hy * st->d2yydy2[j];                    // src/fluxes.cpp:253
+        tmpy2[j] = d.h2y * st->dyydy[j] * st->dyydy[j];      // src/fluxes.cpp:254
+    }
+    std::vector<double> dzzdz(st->dzzdz, st->dzzdz + NZ), d2zzdz2(st->d2zzdz2, st->d2zzdz2 + NZ),
+        ddz(st->ddz, st->ddz + NZ), rkapa(st->rkapa, st->rkapa + NZ), dkapa(st->dkapa, st->dkapa + NZ);
+    std::vector<double> tmpz(NZ), tmpz1(NZ), tmpz2(NZ);
+    for (int64_t k = 0; k < NZ; ++k) {
+        tmpz[k] = d.hz * st->dzzdz[k];                       // src/fluxes.cpp:101
+        tmpz1[k] = d.hz * st->d2zzdz2[k];                    // src/fluxes.cpp:250
+        tmpz2[k] = d.h2z * st->dzzdz[k] * st->dzzdz[k];      // src/fluxes.cpp:251
+    }
+    // plume profile factors (src/bcon.cpp:47-68); host libm, as the reference
+    std::vector<double> px(NX, 0.0), py(NY, 0.0);
+    const double cln = (double)(-4.0f * logf(2.0f)) / (p.hh * p.hh);
+    for (int64_t i = 0; i < NX; ++i) {
+        const double a = st->exx[i] - p.xp;
+        px[i] = (p.itcon == 0) ? std::exp(cln * a * a) : std::exp(cln * (a * a));
+    }
+    for (int64_t j = 0; j < NY; ++j) {
+        const double a = st->wyy[j] - p.yp;
+        py[j] = (p.itcon == 0) ? std::exp(cln * a * a) : std::exp(cln * (a * a));
+    }
+    std::vector<const std::vector<double>*> tabs = {&dxxdx, &d2xxdx2, &ddx,  &dyydy, &tmpy,
+                                                    &tmpy1, &tmpy2,   &ddy,  &dzzdz, &d2zzdz2,
+                                                    &tmpz,  &tmpz1,   &tmpz2, &ddz,  &rkapa,
+                                                    &dkapa, &px,      &py};
+    size_t total = 0;
+    for (auto* t : tabs) total += (t->size() + 15) / 16 * 16;
+    if (!g->line_buf) {
+        cuda_ok(cudaMalloc(&g->line_buf, total * sizeof(double)), "cudaMalloc(lines)");
+        g->bytes += total * sizeof(double);
+    }
+    std::vector<double> packed(total, 0.0);
+    std::vector<const double*> dev;
+    size_t off = 0;
+    for (auto* t : tabs) {
+        std::memcpy(packed.data() + off, t->data(), t->size() * sizeof(double));
+        dev.push_back(g->line_buf + off);
+        off += (t->size() + 15) / 16 * 16;
+    }
+    cuda_ok(cudaMemcpy(g->line_buf, packed.data(), total * sizeof(double), cudaMemcpyHostToDevice),
+            "upload lines");
+    r3dk::Lines& L = g->lines;
+    L.dxxdx = dev[0]; L.d2xxdx2 = dev[1]; L.ddx = dev[2];
+    L.dyydy = dev[3]; L.tmpy = dev[4]; L.tmpy1 = dev[5]; L.tmpy2 = dev[6]; L.ddy = dev[7];
+    L.dzzdz = dev[8]; L.d2zzdz2 = dev[9]; L.tmpz = dev[10]; L.tmpz1 = dev[11]; L.tmpz2 = dev[12];
+    L.ddz = dev[13]; L.rkapa = dev[14]; L.dkapa = dev[15]; L.plume_x = dev[16]; L.plume_y = dev[17];
+    bool kc = true;
+    for (int64_t k = 1; k <= NZ - 2; ++k) kc = kc && rkapa[k] == 1.0 && dkapa[k] == 0.0;
+    g->ph.kappa_const = kc ? 1 : 0;
+    const double dzs = (double)(1.0f / (float)(p.npz - 1));
+    g->bnd.dz_top = dzs / st->dzzdz[1];            // src/bcon.cpp:59
+    g->bnd.dz_bot = dzs / st->dzzdz[p.npz];        // src/bcon.cpp:124
+}
+
+}  // namespace
+
+extern "C" {
+
+int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
+    return guarded([&] {
+        if (!p || !out) throw std::invalid_argument("null argument");
+        *out = nullptr;
+        check_params(*p);
+        auto g = new r3d_gpu();
+        try {
+            g->p = *p;
+            g->d = derive(*p);
+            g->device = p->gpu_id;
+            int ndev = 0;
+            cuda_ok(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+            if (g->device < 0 || g->device >= ndev) throw std::invalid_argument("--gpu id out of range");
+            DeviceGuard dg(g->device);
+            cuda_ok(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            const Derived& d = g->d;
+            g->nfields = p->lmag ? 8 : 5;
+            g->geo.npx = p->npx;
+            g->geo.npy = p->npy;
+            g->geo.npz = p->npz;
+            g->geo.pitch = (d.nx + 15) / 16 * 16;
+            g->geo.plane = g->geo.pitch * d.ny;
+            const size_t nbytes = (size_t)g->geo.plane * d.nz * sizeof(double);
+            for (int b = 0; b < 2; ++b)
+                for (int q = 0; q < g->nfields; ++q) {
+                    cuda_ok(cudaMalloc(&g->X[b][q], nbytes), "cudaMalloc(state)");
+                    g->bytes += nbytes;
+                }
+            for (int q = 0; q < g->nfields; ++q) {
+                cuda_ok(cudaMalloc(&g->Z[q], nbytes), "cudaMalloc(accumulator)");
+                cuda_ok(cudaMemsetAsync(g->Z[q], 0, nbytes, g->stream), "cudaMemset");
+                g->bytes += nbytes;
+            }
+            cuda_ok(cudaMalloc(&g->dsc, sizeof(r3dk::Scalars)), "cudaMalloc(scalars)");
+            cuda_ok(cudaMallocHost(&g->hsc, sizeof(r3dk::Scalars)), "cudaMallocHost");
+            r3dk::Physics& ph = g->ph;
+            ph.hx = d.hx; ph.h2x = d.h2x; ph.hy = d.hy; ph.hz = d.hz;
+            ph.c13 = d.c13; ph.c23 = d.c23; ph.c43 = d.c43; ph.ore = d.ore; ph.ocv = d.ocv;
+            ph.grav = p->grav;
+            ph.tdiff = d.ocv / d.repr;
+            ph.theat = d.ocv * d.ore;
+            ph.theat43 = d.c43 * d.ocv * d.ore;
+            ph.t13 = d.c13 * d.ore;
+            ph.omx = d.omx; ph.omz = d.omz;
+            ph.gamma = p->gamma; ph.ogamma = 1.0 / p->gamma; ph.re = p->re; ph.repr = d.repr;
+            ph.cv = d.cv; ph.rm = p->rm; ph.obeta = d.obeta; ph.orm = d.orm; ph.sff = p->sf;
+            for (int s = 0; s < 3; ++s) { ph.gam[s] = d.gam[s]; ph.zeta[s] = d.zeta[s]; }
+            ph.lrot = p->lrot; ph.lmag = p->lmag;
+            ph.kappa_const = 1;
+            r3dk::Boundary& b = g->bnd;
+            if (p->tp != 0.0 && (p->itcon == 0 || p->itcon == 1)) b.top_mode = p->itcon == 0 ? 2 : 3;
+            else if (p->itcon == 4) b.top_mode = 4;
+            else b.top_mode = p->itcon == 0 ? 0 : 1;
+            b.bottom_mode = p->izcon;
+            b.hh = p->hh; b.theta = p->theta; b.tp = p->tp; b.tpr = p->tp;
+            b.half_nx = (int)(d.nx / 2);
+            g->kchunk = p->npz >= 256 ? 32 : 16;
+            cuda_ok(cudaStreamSynchronize(g->stream), "create");
+        } catch (...) {
+            r3d_gpu_destroy(g);
+            throw;
+        }
+        *out = g;
+    });
+}
+
+int r3d_gpu_destroy(r3d_gpu* g) {
+    if (!g) return R3D_OK;
+    DeviceGuard dg(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    for (int b = 0; b < 2; ++b)
+        for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->X[b][q]);
+    for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->Z[q]);
+    cudaFree(g->line_buf);
+    cudaFree(g->dsc);
+    if (g->hsc) cudaFreeHost(g->hsc);
+    for (auto e : g->ev) cudaEventDestroy(e);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return R3D_OK;
+}
+
+int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) {
+    return guarded([&] {
+        if (!g || !st || !sc) throw std::invalid_argument("null argument");
+        DeviceGuard dg(g->device);
+        const Derived& d = g->d;
+        const double* src[r3dk::kMaxFields] = {st->ru, st->rv, st->rw, st->ro, st->tt, st->bx, st->by, st->bz};
+        for (int q = 0; q < g->nfields; ++q)
+            if (!src[q]) throw std::invalid_argument("r3d_host_state field is NULL");
+        const double* lines[] = {st->dxxdx, st->d2xxdx2, st->ddx, st->exx, st->dyydy, st->d2yydy2,
+                                 st->ddy, st->wyy, st->dzzdz, st->d2zzdz2, st->ddz, st->rkapa, st->dkapa};
+        for (auto l : lines)
+            if (!l) throw std::invalid_argument("r3d_host_state metric line is NULL");
+        upload_lines(g, st);
+        for (int b = 0; b < 2; ++b)
+            for (int q = 0; q < g->nfields; ++q)
+                cuda_ok(cudaMemcpy2DAsync(g->X[b][q], g->geo.pitch * sizeof(double), src[q],
+                                          d.nx * sizeof(double), d.nx * sizeof(double), d.ny * d.nz,
+                                          cudaMemcpyHostToDevice, g->stream),
+                        "upload state");
+        g->cur = 0;
+        r3dk::Scalars h{};
+        h.dt = sc->dt; h.timc = sc->timc; h.timt = sc->timt; h.timi = sc->timi;
+        h.umach = sc->umach; h.tb = sc->tb; h.nit = sc->nit;
+        *g->hsc = h;
+        cuda_ok(cudaMemcpyAsync(g->dsc, g->hsc, sizeof(h), cudaMemcpyHostToDevice, g->stream), "upload scalars");
+        g->bnd.tb = sc->tb;
+        g->host_timc = sc->timc;
+        g->host_timi = sc->timi;
+        cuda_ok(r3dk::launch_reset_reduction(g->dsc, g->stream), "reset");
+        FieldSet fs = fieldset(g);
+        cuda_ok(r3dk::launch_dt_full(g->geo, g->ph, g->lines, fs, g->dsc, g->stream), "dt_full");
+        cuda_ok(cudaStreamSynchronize(g->stream), "upload");
+        g->uploaded = true;
+    });
+}
+
+int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc) {
+    return guarded([&] {
+        if (!g || !st) throw std::invalid_argument("null argument");
+        if (!g->uploaded) throw Error(R3D_ESTATE, "download before upload");
+        DeviceGuard dg(g->device);
+        const Derived& d = g->d;
+        double* dst[r3dk::kMaxFields] = {st->ru, st->rv, st->rw, st->ro, st->tt, st->bx, st->by, st->bz};
+        for (int q = 0; q < g->nfields; ++q) {
+            if (!dst[q]) continue;
+            cuda_ok(cudaMemcpy2DAsync(dst[q], d.nx * sizeof(double), g->X[g->cur][q],
+                                      g->geo.pitch * sizeof(double), d.nx * sizeof(double), d.ny * d.nz,
+                                      cudaMemcpyDeviceToHost, g->stream),
+                    "download state");
+        }
+        pull_scalars(g, sc);
+    });
+}
+
+int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes) {
+    if (!g || !bytes) return R3D_EINVAL;
+    *bytes = g->bytes;
+    return R3D_OK;
+}
+
+void* r3d_gpu_stream(r3d_gpu* g) { return g ? (void*)g->stream : nullptr; }
+
+int r3d_gpu_step(r3d_gpu* g, int nstages, r3d_scalars* sc) {
+    return guarded([&] {
+        if (!g) throw std::invalid_argument("null handle");
+        if (nstages < 1 || nstages > 3) throw std::invalid_argument("nstages must be 1..3");
+        if (!g->uploaded) throw Error(R3D_ESTATE, "step before upload");
+        DeviceGuard dg(g->device);
+        Timer tm{g, false, nullptr};
+        int a = 0, b = 0;
+        enqueue_step(g, nstages, tm, a, b);
+        r3d_scalars tmp{};
+        pull_scalars(g, &tmp);
+        if (sc) *sc = tmp;
+        if (!std::isfinite(tmp.dt)) throw Error(R3D_ENUMERIC, "non-finite dt");
+    });
+}
+
+int r3d_gpu_run(r3d_gpu* g, int nsteps, r3d_scalars* sc) {
+    return guarded([&] { run_steps(g, nsteps, sc, nullptr, true); });
+}
+
+int r3d_gpu_enqueue(r3d_gpu* g, int nsteps) {
+    return guarded([&] { run_steps(g, nsteps, nullptr, nullptr, false); });
+}
+
+int r3d_gpu_run_timed(r3d_gpu* g, int nsteps, r3d_scalars* sc, r3d_timing* tm) {
+    return guarded([&] {
+        if (!tm) throw std::invalid_argument("null timing");
+        run_steps(g, nsteps, sc, tm, true);
+    });
+}
+
+int r3d_gpu_totals(r3d_gpu* g, double* mass, double* energy) {
+    return guarded([&] {
+        if (!g || !g->uploaded) throw Error(R3D_ESTATE, "totals before upload");
+        DeviceGuard dg(g->device);
+        double zero[2] = {0.0, 0.0};
+        cuda_ok(cudaMemcpyAsync(&g->dsc->mass, zero, sizeof(zero), cudaMemcpyHostToDevice, g->stream), "totals");
+        FieldSet fs = fieldset(g);
+        cuda_ok(r3dk::launch_totals(g->geo, g->ph, fs, g->dsc, g->stream), "totals");
+        cuda_ok(cudaMemcpyAsync(zero, &g->dsc->mass, sizeof(zero), cudaMemcpyDeviceToHost, g->stream), "totals");
+        cuda_ok(cudaStreamSynchronize(g->stream), "totals");
+        if (mass) *mass = zero[0];
+        if (energy) *energy = zero[1];
+    });
+}
+
+}  // extern "C"

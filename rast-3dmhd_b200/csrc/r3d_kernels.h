@@ -1,0 +1,41 @@
+// r3d_kernels.h - launchers of the step kernels (host side of csrc/*.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "r3d_device.cuh"
+
+namespace r3dk {
+
+// Field pointers of one stage: the state read (xin), the state written (xout) and the RK
+// accumulator read/written in place (z); order ru rv rw ro tt bx by bz.
+struct FieldSet {
+    const double* xin[kMaxFields];
+    double* xout[kMaxFields];
+    double* z[kMaxFields];
+};
+
+// FP32-bulk field pointers: thermodynamic deviations and momenta stored as float.
+struct FieldSet32 {
+    const float* xin[5];
+    float* xout[5];
+    float* z[5];
+};
+
+size_t stage_fp64_smem();
+cudaError_t launch_stage_fp64(int stage, const Geometry& g, const Physics& ph, const Lines& L,
+                              const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st);
+cudaError_t launch_stage_mhd_fp64(int stage, const Geometry& g, const Physics& ph,
+                                  const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk,
+                                  cudaStream_t st);
+cudaError_t launch_bcon(const Geometry& g, const Physics& ph, const Lines& L, const Boundary& b,
+                        const FieldSet& fs, Scalars* sc, int with_dt, cudaStream_t st);
+cudaError_t launch_dt_full(const Geometry& g, const Physics& ph, const Lines& L,
+                           const FieldSet& fs, Scalars* sc, cudaStream_t st);
+cudaError_t launch_step_begin(const Physics& ph, Scalars* sc, cudaStream_t st);
+cudaError_t launch_step_end(Scalars* sc, cudaStream_t st);
+cudaError_t launch_reset_reduction(Scalars* sc, cudaStream_t st);
+cudaError_t launch_totals(const Geometry& g, const Physics& ph, const FieldSet& fs, Scalars* sc,
+                          cudaStream_t st);
+
+}  // namespace r3dk

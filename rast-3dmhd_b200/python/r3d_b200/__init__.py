@@ -1,0 +1,277 @@
+"""Python binding of the B200 Rast-3DMHD step (ctypes over include/r3d_gpu.h).
+
+This is the host-side mirror of the reference's driver interface (src/main.cpp:125-275): parse
+the reference command line into a parameter struct, build the initial state on the host,
+upload it, step on the GPU, download.  All compute runs in lib/librast3d_b200.so; there is no
+Python or CPU fallback: if the library is missing or no CUDA device is present the calls
+raise.
+
+    p = r3d_b200.parse(["--npx", "32", "--npy", "32", "--npz", "64"])
+    st = r3d_b200.HostState.setup(p)          # metrics + static IC (host, once)
+    sim = r3d_b200.GpuSim(p)                   # gpu_alloc
+    sim.upload(st)                             # gpu_upload
+    sc = sim.step()                            # step_gpu: dt, timc, nit, ...
+    sim.download(st)                           # gpu_download
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+LIB_PATH = os.path.join(_PKG, "lib", "librast3d_b200.so")
+
+R3D_OK, R3D_EINVAL, R3D_ECUDA, R3D_ENOMEM, R3D_ESTATE, R3D_ENUMERIC = 0, -1, -2, -3, -4, -5
+PREC_FP64, PREC_FP32BULK = 0, 1
+
+_INTS1 = ["npx", "npy", "npz", "npey", "ix", "iy", "ilap", "ipad", "ngrid", "id", "ncol", "nrow",
+          "ixcon", "iycon", "izcon", "itcon", "ibcon", "lrot", "lmag", "lpot", "lrem", "lshr",
+          "ncase", "ncasep", "ntotal", "nstep0", "nstart", "ntube"]
+_DBLS = ["re", "pr", "theta", "grav", "r_y", "ang", "rm", "beta", "pzp", "sigma", "polys", "tp",
+         "tc", "xp", "yp", "zp", "xmax", "ymax", "zmax", "ampt", "ampb", "bfh", "bzp", "qfh",
+         "gamma", "hh", "dh", "dv", "tstart", "toff", "rlax", "xx1", "xx2", "yy1", "yy2", "zz1",
+         "zz2", "xa", "xb", "xc", "xd", "ya", "yb", "yc", "yd", "za", "zb", "zc", "zd", "xcent",
+         "zcent", "rmax", "cmt", "a_tube", "lambda", "vz0", "sf"]
+_INTS2 = ["backend", "gpu_id", "seed", "precision"]
+
+
+class Params(ctypes.Structure):
+    """r3d_params (mirrors the reference Params, include/params.hpp:24-120)."""
+    _fields_ = ([(n, ctypes.c_int) for n in _INTS1] + [(n, ctypes.c_double) for n in _DBLS]
+                + [(n, ctypes.c_int) for n in _INTS2])
+
+    def as_dict(self) -> Dict[str, float]:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class Scalars(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("timc", ctypes.c_double), ("timt", ctypes.c_double),
+                ("timi", ctypes.c_double), ("umach", ctypes.c_double), ("tb", ctypes.c_double),
+                ("nit", ctypes.c_int)]
+
+    def as_dict(self) -> Dict[str, float]:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+FIELDS3D = ["ru", "rv", "rw", "ro", "tt", "bx", "by", "bz"]
+LINES = ["exx", "dxxdx", "d2xxdx2", "ddx", "wyy", "dyydy", "d2yydy2", "ddy",
+         "zee", "dzzdz", "d2zzdz2", "ddz", "rkapa", "dkapa"]
+
+
+class _HostStateC(ctypes.Structure):
+    _fields_ = [(n, ctypes.POINTER(ctypes.c_double)) for n in FIELDS3D + LINES]
+
+
+class Timing(ctypes.Structure):
+    _fields_ = [("total_ms", ctypes.c_double), ("stage_ms", ctypes.c_double),
+                ("bcon_ms", ctypes.c_double), ("other_ms", ctypes.c_double),
+                ("stage_launches", ctypes.c_int), ("total_launches", ctypes.c_int)]
+
+
+class R3dError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"r3d error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load librast3d_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} not built; run __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip = ctypes.c_void_p, ctypes.c_int
+        L.r3d_params_default.argtypes = [ctypes.POINTER(Params)]
+        L.r3d_params_parse.argtypes = [ip, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(Params)]
+        L.r3d_params_check.argtypes = [ctypes.POINTER(Params)]
+        L.r3d_derived_get.argtypes = [ctypes.POINTER(Params), ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+        L.r3d_dims.argtypes = [ctypes.POINTER(Params)] + [ctypes.POINTER(ctypes.c_int64)] * 3
+        L.r3d_setup_host.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(_HostStateC), ctypes.POINTER(Scalars)]
+        L.r3d_static_profile.argtypes = [ctypes.POINTER(Params), vp, vp]
+        L.r3d_gpu_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(vp)]
+        L.r3d_gpu_upload.argtypes = [vp, ctypes.POINTER(_HostStateC), ctypes.POINTER(Scalars)]
+        L.r3d_gpu_download.argtypes = [vp, ctypes.POINTER(_HostStateC), ctypes.POINTER(Scalars)]
+        L.r3d_gpu_destroy.argtypes = [vp]
+        L.r3d_gpu_memory.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.r3d_gpu_stream.argtypes = [vp]
+        L.r3d_gpu_stream.restype = vp
+        L.r3d_gpu_step.argtypes = [vp, ip, ctypes.POINTER(Scalars)]
+        L.r3d_gpu_run.argtypes = [vp, ip, ctypes.POINTER(Scalars)]
+        L.r3d_gpu_enqueue.argtypes = [vp, ip]
+        L.r3d_gpu_run_timed.argtypes = [vp, ip, ctypes.POINTER(Scalars), ctypes.POINTER(Timing)]
+        L.r3d_gpu_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.r3d_last_error.restype = ctypes.c_char_p
+        L.r3d_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != R3D_OK:
+        raise R3dError(rc, lib().r3d_last_error().decode())
+
+
+def default_params() -> Params:
+    p = Params()
+    _check(lib().r3d_params_default(ctypes.byref(p)))
+    return p
+
+
+def parse(args: Sequence[str], base: Optional[Params] = None) -> Params:
+    """Reference command line (src/params.cpp:113-224) + --seed/--precision -> Params."""
+    p = default_params() if base is None else base
+    arr = (ctypes.c_char_p * max(1, len(args)))(*[a.encode() for a in args])
+    _check(lib().r3d_params_parse(len(args), arr, ctypes.byref(p)))
+    return p
+
+
+def check(p: Params):
+    _check(lib().r3d_params_check(ctypes.byref(p)))
+
+
+def derived(p: Params, name: str) -> float:
+    out = ctypes.c_double()
+    _check(lib().r3d_derived_get(ctypes.byref(p), name.encode(), ctypes.byref(out)))
+    return out.value
+
+
+def dims(p: Params):
+    n = [ctypes.c_int64() for _ in range(3)]
+    _check(lib().r3d_dims(ctypes.byref(p), *[ctypes.byref(x) for x in n]))
+    return tuple(int(x.value) for x in n)
+
+
+def static_profile(p: Params):
+    t = np.zeros(p.npz)
+    r = np.zeros(p.npz)
+    _check(lib().r3d_static_profile(ctypes.byref(p), t.ctypes.data, r.ctypes.data))
+    return t, r
+
+
+@dataclass
+class HostState:
+    """Host arrays on the global domain, shapes (NZ, NY, NX) and (N,) for lines."""
+    fields: Dict[str, np.ndarray]
+    lines: Dict[str, np.ndarray]
+    scalars: Dict[str, float]
+
+    @classmethod
+    def empty(cls, p: Params) -> "HostState":
+        NX, NY, NZ = dims(p)
+        names = FIELDS3D if p.lmag else FIELDS3D[:5]
+        fields = {n: np.zeros((NZ, NY, NX)) for n in names}
+        lines = {}
+        for q, n in enumerate(LINES):
+            lines[n] = np.zeros(NX if q < 4 else (NY if q < 8 else NZ))
+        return cls(fields, lines, {})
+
+    @classmethod
+    def setup(cls, p: Params) -> "HostState":
+        """Grid metrics, conductivity, static IC, seeded perturbation, periodic ghosts."""
+        st = cls.empty(p)
+        sc = Scalars()
+        c = st._c()
+        _check(lib().r3d_setup_host(ctypes.byref(p), ctypes.byref(c), ctypes.byref(sc)))
+        st.scalars = sc.as_dict()
+        return st
+
+    def _c(self) -> _HostStateC:
+        c = _HostStateC()
+        dp = ctypes.POINTER(ctypes.c_double)
+        for n in FIELDS3D:
+            a = self.fields.get(n)
+            if a is not None:
+                assert a.flags.c_contiguous and a.dtype == np.float64
+                setattr(c, n, a.ctypes.data_as(dp))
+        for n in LINES:
+            a = self.lines[n]
+            setattr(c, n, a.ctypes.data_as(dp))
+        return c
+
+    def copy(self) -> "HostState":
+        return HostState({k: v.copy() for k, v in self.fields.items()},
+                         {k: v.copy() for k, v in self.lines.items()}, dict(self.scalars))
+
+
+class GpuSim:
+    """Device-resident simulation (replaces GpuSim + gpu_alloc/upload/step_gpu/download/free)."""
+
+    def __init__(self, p: Params):
+        self.p = p
+        h = ctypes.c_void_p()
+        _check(lib().r3d_gpu_create(ctypes.byref(p), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().r3d_gpu_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, st: HostState):
+        sc = Scalars(**{k: (int(v) if k == "nit" else v) for k, v in st.scalars.items()})
+        c = st._c()
+        _check(lib().r3d_gpu_upload(self.h, ctypes.byref(c), ctypes.byref(sc)))
+
+    def download(self, st: HostState) -> Dict[str, float]:
+        sc = Scalars()
+        c = st._c()
+        _check(lib().r3d_gpu_download(self.h, ctypes.byref(c), ctypes.byref(sc)))
+        st.scalars = sc.as_dict()
+        return st.scalars
+
+    def step(self, nstages: int = 3) -> Dict[str, float]:
+        sc = Scalars()
+        _check(lib().r3d_gpu_step(self.h, nstages, ctypes.byref(sc)))
+        return sc.as_dict()
+
+    def run(self, nsteps: int) -> Dict[str, float]:
+        sc = Scalars()
+        _check(lib().r3d_gpu_run(self.h, nsteps, ctypes.byref(sc)))
+        return sc.as_dict()
+
+    def enqueue(self, nsteps: int):
+        _check(lib().r3d_gpu_enqueue(self.h, nsteps))
+
+    def run_timed(self, nsteps: int):
+        sc, tm = Scalars(), Timing()
+        _check(lib().r3d_gpu_run_timed(self.h, nsteps, ctypes.byref(sc), ctypes.byref(tm)))
+        return sc.as_dict(), {n: getattr(tm, n) for n, _ in tm._fields_}
+
+    def totals(self):
+        m, e = ctypes.c_double(), ctypes.c_double()
+        _check(lib().r3d_gpu_totals(self.h, ctypes.byref(m), ctypes.byref(e)))
+        return m.value, e.value
+
+    @property
+    def stream(self) -> int:
+        return int(lib().r3d_gpu_stream(self.h) or 0)
+
+    @property
+    def memory_bytes(self) -> int:
+        b = ctypes.c_int64()
+        _check(lib().r3d_gpu_memory(self.h, ctypes.byref(b)))
+        return int(b.value)
+
+
+def version() -> str:
+    return lib().r3d_version().decode()

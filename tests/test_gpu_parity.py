@@ -1,0 +1,108 @@
+"""FP64 GPU step vs the oracle, bit for bit (the reference's own bar: tests/golden_util.hpp:94-104
+compares interiors with max |diff| == 0, and tests/gpu_equivalence_test.cpp:143-174 also
+requires dt and nit to be equal).
+
+Each case builds the initial state with the product's host set-up (itself checked against the
+oracle in test_host.py), steps it on the GPU through the C ABI, and compares the interiors of
+ru rv rw ro tt and the scalars with the C restatement stepped from its own initial state.
+"""
+import numpy as np
+import pytest
+
+import r3d_b200 as R
+from oracle import Oracle, Reference, interior
+
+PRIMARY = ["ru", "rv", "rw", "ro", "tt"]
+
+# (name, flags, seed, steps)
+HYDRO_CASES = [
+    ("config1_32x32x64_seed1", ["--npx", "32", "--npy", "32", "--npz", "64"], 1, 20),
+    ("golden_16x16x32", ["--npx", "16", "--npy", "16", "--npz", "32"], 62659, 3),
+    ("ragged_37x13x23", ["--npx", "37", "--npy", "13", "--npz", "23"], 5, 5),
+    ("ngrid2_izcon1_itcon0", ["--npx", "24", "--npy", "20", "--npz", "36", "--ngrid", "2",
+                              "--izcon", "1", "--itcon", "0"], 5, 5),
+    ("ngrid0_rotation_tc", ["--npx", "24", "--npy", "20", "--npz", "36", "--ngrid", "0",
+                            "--lrot", "1", "--ry", "2", "--ang", "0.3", "--tc", "0.5"], 5, 5),
+    ("variable_kappa", ["--npx", "24", "--npy", "20", "--npz", "36", "--pzp", "0.5",
+                        "--sigma", "0.1", "--polys", "1.5"], 7, 5),
+    ("itcon4", ["--npx", "24", "--npy", "16", "--npz", "40", "--itcon", "4"], 3, 4),
+    ("no_plume", ["--npx", "24", "--npy", "16", "--npz", "40", "--tp", "0"], 3, 4),
+    ("min_size", ["--npx", "3", "--npy", "3", "--npz", "8"], 2, 3),
+]
+
+
+def gpu_run(flags, seed, steps, last_stages=3, use_run=False):
+    p = R.parse(flags + ["--seed", str(seed)])
+    st = R.HostState.setup(p)
+    with R.GpuSim(p) as sim:
+        sim.upload(st)
+        if use_run and last_stages == 3:
+            sc = sim.run(steps)
+        else:
+            sc = None
+            for n in range(steps):
+                sc = sim.step(3 if n < steps - 1 else last_stages)
+        sim.download(st)
+    return st, sc
+
+
+def oracle_run(flags, seed, steps, last_stages=3):
+    o = Oracle(flags).init(seed)
+    for n in range(steps):
+        o.step(3 if n < steps - 1 else last_stages)
+    return o
+
+
+def assert_bitexact(st, o, sc, names=PRIMARY):
+    for n in names:
+        a, b = interior(st.fields[n]), interior(o.field(n))
+        diff = float(np.abs(a - b).max())
+        assert diff == 0.0, f"{n}: max |gpu - oracle| = {diff:.3e}"
+    osc = o.scalars()
+    for k in ("dt", "timc", "timt", "umach"):
+        assert sc[k] == osc[k], f"{k}: gpu {sc[k]!r} oracle {osc[k]!r}"
+    assert sc["nit"] == int(osc["nit"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,flags,seed,steps", HYDRO_CASES, ids=[c[0] for c in HYDRO_CASES])
+def test_hydro_steps_bitexact(name, flags, seed, steps):
+    st, sc = gpu_run(flags, seed, steps)
+    o = oracle_run(flags, seed, steps)
+    assert_bitexact(st, o, sc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("stages", [1, 2, 3])
+def test_partial_step_bitexact(stages):
+    """step(nstages) for the per-stage bisection the reference tests use
+    (tests/gpu_equivalence_test.cpp:178-332)."""
+    flags = ["--npx", "32", "--npy", "24", "--npz", "48"]
+    st, sc = gpu_run(flags, 11, 2, last_stages=stages)
+    o = oracle_run(flags, 11, 2, last_stages=stages)
+    assert_bitexact(st, o, sc)
+
+
+@pytest.mark.gpu
+def test_run_matches_step_loop():
+    """r3d_gpu_run (device-resident loop) equals repeated r3d_gpu_step."""
+    flags = ["--npx", "40", "--npy", "24", "--npz", "48"]
+    a, sa = gpu_run(flags, 9, 6)
+    b, sb = gpu_run(flags, 9, 6, use_run=True)
+    for n in PRIMARY:
+        assert np.array_equal(interior(a.fields[n]), interior(b.fields[n])), n
+    assert sa == sb
+
+
+@pytest.mark.gpu
+def test_gpu_vs_reference_build_directly():
+    """When the reference CPU build is present, also compare against it without the oracle."""
+    if not Reference.available():
+        pytest.skip("reference build not present")
+    flags = ["--npx", "32", "--npy", "32", "--npz", "64"]
+    st, sc = gpu_run(flags, 1, 20)
+    rf, _, rs, _ = Reference.run(flags + ["--npey", "1"], nranks=2, seed=1, nsteps=20, omp_threads=4)
+    for n in PRIMARY:
+        assert float(np.abs(interior(st.fields[n]) - interior(rf[n])).max()) == 0.0, n
+    for k in ("dt", "timc", "umach"):
+        assert sc[k] == rs[k], k
