@@ -1,0 +1,330 @@
+"""Benchmark: Rast-3DMHD FP64 RK3 step on B200, in Mcell-updates/s.
+
+Workload (one "step" = one full RK3 time step, dt reduction, BCON and ghost fill included):
+FP64 hydro on the 504 x 504 x 512 grid with default physics (re=2 pr=0.05 theta=0.25
+grav=0.625 gamma=5/3 sff=0.315, ngrid=1, plume top BC), polytropic static IC with the RAN2
+temperature perturbation (amplitude 0.005) drawn with seed 3.  Inputs are synthetic (no
+dataset exists for this path); the working set (15 x 1.07 GB) is far larger than L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Timing: W untimed steps, then K steps timed with CUDA events recorded by the library on the
+stream its kernels run on (every launch is bracketed, which also yields the per-kernel
+durations for the roofline); barrier + device synchronise on both sides; max over ranks.
+Under torchrun each rank runs its own replica of the workload (the single-GPU form keeps the
+whole domain on one device; slab decomposition over GPUs is not part of this build).
+The reference arm (--impl reference) times the reference's own CPU sources (compiled
+unmodified into oracle/_ref) on a bounded slab of the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "rast-3dmhd_b200", "python"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+GRID = (504, 504, 512)
+SEED = 3
+FLAGS = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(GRID[2])]
+METRIC = "Mcell-updates/s per RK3 step (FP64, bit-exact vs reference CPU)"
+UNIT = "Mcell-updates/s"
+# algorithmic HBM bytes per interior cell: stage 1 reads X (5 fields) and writes X', Z'
+# (10); stage 2 reads X, Z and writes X', Z' (20); stage 3 reads X, Z and writes X' (15):
+# 50 field passes x 8 B per step, i.e. 400 B/cell/step and 400/3 B per cell per stage launch.
+BYTES_PER_CELL_STEP = 400.0
+BYTES_PER_CELL_STAGE = BYTES_PER_CELL_STEP / 3.0
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "stage_fp64_504x504x64.md")
+
+
+def peak_hbm():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def stage_traffic_per_launch(cells: int):
+    """DRAM bytes per stage launch from the committed ncu summary (scaled by cells), or None."""
+    try:
+        with open(TRAFFIC_FILE) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_cell_per_stage_launch:"):
+                    return float(line.split(":", 1)[1]) * cells
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def allmax(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_sample(max_seconds: float = 20.0):
+    """Time the reference CPU sources (or the oracle port when absent) on a slab of the
+    workload: full 504 x 504 plane, reduced depth, same physics and seed."""
+    import numpy as np  # noqa: F401
+
+    ncores = os.cpu_count() or 1
+    nz = 16
+    args = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(nz), "--npey", "1"]
+    cells = GRID[0] * GRID[1] * nz
+    try:
+        from oracle import Reference
+
+        if not Reference.available():
+            raise RuntimeError("reference build absent")
+        ranks = 2
+        threads = max(1, ncores // ranks)
+        # warm-up + calibration with one step, then as many as fit the budget
+        _, _, _, s1 = Reference.run(args, nranks=ranks, seed=SEED, nsteps=1, omp_threads=threads)
+        nsteps = max(1, min(10, int(max_seconds / max(s1, 1e-3))))
+        _, _, _, sec = Reference.run(args, nranks=ranks, seed=SEED, nsteps=nsteps, omp_threads=threads)
+        return {"value": cells * nsteps / sec / 1e6, "unit": UNIT, "cores": ranks * threads,
+                "kind": "reference",
+                "sample": f"reference CPU sources (src/*.cpp, -O2 -ffp-contract=off -fopenmp) with a "
+                          f"thread-rank MPI stand-in, {ranks} ranks x {threads} OpenMP threads, "
+                          f"grid {GRID[0]}x{GRID[1]}x{nz} (the 504x504 plane at reduced depth), "
+                          f"{nsteps} RK3 steps, seed {SEED}, host has {ncores} logical cores"}
+    except Exception as e:  # oracle port as the stand-in
+        from oracle import Oracle
+
+        o = Oracle(args[:6]).init(SEED)
+        o.step()
+        t0 = time.perf_counter()
+        nsteps = 0
+        while time.perf_counter() - t0 < max_seconds / 2 and nsteps < 10:
+            o.step()
+            nsteps += 1
+        sec = time.perf_counter() - t0
+        return {"value": cells * nsteps / sec / 1e6, "unit": UNIT, "cores": ncores, "kind": "port",
+                "sample": f"C restatement (oracle/r3d_oracle.c, OpenMP) on {GRID[0]}x{GRID[1]}x{nz}, "
+                          f"{nsteps} steps ({e})"}
+
+
+def run_reference_arm(args, world, rank, pg):
+    if rank != 0:
+        return 0
+    base = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "impl": "reference"}
+    try:
+        from oracle import Reference
+
+        if not Reference.available():
+            print(json.dumps({**base, "impl": "reference",
+                              "unavailable": "reference CPU build oracle/_ref/libr3dref.so not present"}))
+            return 0
+        ncores = os.cpu_count() or 1
+        nz = 16
+        fl = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(nz), "--npey", "1"]
+        cells = GRID[0] * GRID[1] * nz
+        ranks, threads = 2, max(1, ncores // 2)
+        Reference.run(fl, nranks=ranks, seed=SEED, nsteps=max(1, args.warmup // 3), omp_threads=threads)
+        nsteps = max(1, min(args.steps, 10))
+        _, _, _, sec = Reference.run(fl, nranks=ranks, seed=SEED, nsteps=nsteps, omp_threads=threads)
+        v = cells * nsteps / sec / 1e6
+        sample = (f"reference CPU sources compiled unmodified (-O2 -ffp-contract=off -fopenmp), "
+                  f"{ranks} thread-ranks x {threads} OpenMP threads, grid {GRID[0]}x{GRID[1]}x{nz} "
+                  f"(504x504 plane, reduced depth), {nsteps} timed RK3 steps, seed {SEED}")
+        out = {**base, "value": v, "ms_per_step": sec / nsteps * 1e3, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64", "data": "synthetic",
+               "config": {"workload": f"FP64 hydro {GRID[0]}x{GRID[1]}x{GRID[2]} default physics seed {SEED}",
+                          "sample_grid": f"{GRID[0]}x{GRID[1]}x{nz}"},
+               "cpu_baseline": {"value": v, "unit": UNIT, "cores": ranks * threads, "kind": "reference",
+                                "sample": sample},
+               "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+    except Exception as e:
+        print(json.dumps({**base, "unavailable": f"reference CPU run failed: {e}"}))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local, pg = dist_init()
+    if args.impl == "reference":
+        rc = run_reference_arm(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return rc
+
+    import numpy as np
+
+    import r3d_b200 as R
+
+    p = R.parse(FLAGS + ["--seed", str(SEED), "--gpu", str(local)])
+    cells = GRID[0] * GRID[1] * GRID[2]
+    st = R.HostState.setup(p)
+    sim = R.GpuSim(p)
+    sim.upload(st)
+    sim.run(args.warmup)                         # untimed warm-up
+    barrier(pg)
+    with ClockSampler(local) as clk:
+        sc, tm = sim.run_timed(args.steps)       # synchronises on exit
+    barrier(pg)
+    total_ms = allmax(pg, tm["total_ms"])
+    stage_avg_ms = tm["stage_ms"] / max(1, tm["stage_launches"])
+    ms_per_step = total_ms / args.steps
+    value = world * cells * args.steps / (total_ms / 1e3) / 1e6
+
+    # end to end through the C ABI with host buffers: upload from pinned host memory, K steps
+    # that each return the scalars to the host (as step_gpu does), download of the state.
+    import torch
+
+    pinned = {}
+    for n, a in st.fields.items():
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=torch.cuda.is_available())
+        t.numpy()[...] = a
+        pinned[n] = t
+    st_pinned = R.HostState({n: t.numpy() for n, t in pinned.items()}, st.lines, dict(st.scalars))
+    e2e_steps = args.steps
+    barrier(pg)
+    t0 = time.perf_counter()
+    sim.upload(st_pinned)
+    for _ in range(e2e_steps):
+        sim.step()
+    sim.download(st_pinned)
+    e2e_s = allmax(pg, time.perf_counter() - t0)
+    state_bytes = sum(a.nbytes for a in st.fields.values())
+    e2e = {"value": world * cells * e2e_steps / e2e_s / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": int(state_bytes / e2e_steps) + 64,
+           "d2h_bytes_per_step": int(state_bytes / e2e_steps) + 64,
+           "note": "host state uploaded once and downloaded once per K-step job through the C ABI "
+                   "(gpu_upload/step_gpu/gpu_download pattern); bytes amortised per step, plus the "
+                   "per-step scalar read-back"}
+
+    peak, peak_kind = peak_hbm()
+    alg_bytes_launch = cells * BYTES_PER_CELL_STAGE
+    achieved = alg_bytes_launch / (stage_avg_ms / 1e3) / 1e9
+    traffic = stage_traffic_per_launch(cells)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": "stage_hydro_fp64 (fused FLUXES + RK3 stage update)",
+                "step_frac": (cells * BYTES_PER_CELL_STEP / (ms_per_step / 1e3) / 1e9) / peak}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        cpu = cpu_reference_sample()
+    sim.close()
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": f"FP64 hydro {GRID[0]}x{GRID[1]}x{GRID[2]}, default physics, "
+                                      f"polytrope + RAN2 seed {SEED} ampt 0.005",
+                          "grid": list(GRID), "precision": "fp64", "bit_exact": True,
+                          "l2": "inputs 16 GB >> 126 MB L2 (no flush needed)",
+                          "parallelism": f"{world} replica(s), one GPU each"},
+               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+               "gpu_launches": int(tm["total_launches"]), "clocks": clk.summary(),
+               "final_dt": sc["dt"]}
+        print(json.dumps(out))
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

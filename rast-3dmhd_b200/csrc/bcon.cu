@@ -1,0 +1,188 @@
+// bcon.cu - BCON, ghost images, time-step limits and scalar bookkeeping kernels.
+//
+// BCON (src/bcon.cpp:12-141) rewrites planes 1 and npz after every stage; after the third stage
+// it also evaluates the time-step limits of those two planes (the stage kernel covers the
+// others).  dt_full evaluates the limits of a whole state (after an upload or a partial step).
+// step_begin/step_end keep dt, umach, nit, timc, timt on the device (src/step.cpp:133-256).
+#include <cuda_runtime.h>
+
+#include "r3d_kernels.h"
+#include "stage_common.cuh"
+
+namespace r3dk {
+
+// ---------------------------------------------------------------------------------------
+// BCON (src/bcon.cpp:12-141) on planes 1 and npz, their ghost images, and (after the third
+// stage) the time-step limits of those two planes.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) bcon_kernel(Geometry g, Physics ph, Lines L, Boundary b,
+                                                   FieldSet fs, Scalars* sc, int with_dt) {
+    __shared__ double red[5 * 8];
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const bool active = (i <= g.npx) && (j <= g.npy);
+    double m1 = 1e300, m2 = 1e300, m3 = 1e300, m4 = 1e300, mu = 0.0;
+    if (active) {
+        double* ru = fs.xout[0];
+        double* rv = fs.xout[1];
+        double* rw = fs.xout[2];
+        double* ro = fs.xout[3];
+        double* tt = fs.xout[4];
+        const double c13 = ph.c13, c23 = ph.c23, c43 = ph.c43;
+        const int64_t P = g.plane, row = (int64_t)j * g.pitch + i;
+        // top, k = 1 (src/bcon.cpp:27-98)
+        {
+            const int64_t n = P + row;
+            const double ro1 = ro[n], ro2 = ro[n + P], ro3 = ro[n + 2 * P];
+            const double u = ro1 * (c43 * ru[n + P] / ro2 - c13 * ru[n + 2 * P] / ro3);
+            const double v = ro1 * (c43 * rv[n + P] / ro2 - c13 * rv[n + 2 * P] / ro3);
+            double t;
+            switch (b.top_mode) {
+                case 0: t = 1.0; break;
+                case 1: t = c43 * tt[n + P] - c13 * tt[n + 2 * P] - c23 * b.dz_top * b.theta; break;
+                case 2: t = 1.0 - (1.0 - b.tpr) * L.plume_x[i] / b.hh * L.plume_y[j] / b.hh; break;
+                case 3:
+                    t = c43 * tt[n + P] - c13 * tt[n + 2 * P] -
+                        c23 * b.dz_top * (b.theta - (b.theta - b.tpr) * L.plume_x[i] / b.hh * L.plume_y[j] / b.hh);
+                    break;
+                default: t = (i <= b.half_nx) ? 1.0 - b.tp : 1.0; break;
+            }
+            put_periodic(ru, P, g, i, j, u);
+            put_periodic(rv, P, g, i, j, v);
+            put_periodic(rw, P, g, i, j, 0.0);
+            put_periodic(tt, P, g, i, j, t);
+            double b2 = 0.0;
+            if (ph.lmag) {
+                put_periodic(fs.xout[7], P, g, i, j, 0.0);
+                const double bx = fs.xout[5][n], by = fs.xout[6][n];
+                b2 = bx * bx + by * by + 0.0 * 0.0;
+            }
+            if (with_dt) {
+                const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[1]);
+                double w1, w2, w3, w4, um;
+                dt_terms(ph, u, v, 0.0, ro1, t, b2, dd, L.rkapa[1], w1, w2, w3, w4, um);
+                m1 = fold_min(m1, w1); m2 = fold_min(m2, w2); m3 = fold_min(m3, w3);
+                m4 = fold_min(m4, w4); mu = fold_max(mu, um);
+            }
+        }
+        // bottom, k = npz (src/bcon.cpp:104-139)
+        {
+            const int64_t n = (int64_t)g.npz * P + row;
+            const double ro1 = ro[n], ro2 = ro[n - P], ro3 = ro[n - 2 * P];
+            const double u = ro1 * (c43 * ru[n - P] / ro2 - c13 * ru[n - 2 * P] / ro3);
+            const double v = ro1 * (c43 * rv[n - P] / ro2 - c13 * rv[n - 2 * P] / ro3);
+            double t;
+            if (b.bottom_mode == 0)
+                t = b.tb;
+            else
+                t = c43 * tt[n - P] - c13 * tt[n - 2 * P] + c23 * b.dz_bot * b.theta / L.rkapa[g.npz];
+            const int64_t base = (int64_t)g.npz * P;
+            put_periodic(ru, base, g, i, j, u);
+            put_periodic(rv, base, g, i, j, v);
+            put_periodic(rw, base, g, i, j, 0.0);
+            put_periodic(tt, base, g, i, j, t);
+            double b2 = 0.0;
+            if (ph.lmag) {
+                put_periodic(fs.xout[7], base, g, i, j, 0.0);
+                const double bx = fs.xout[5][n], by = fs.xout[6][n];
+                b2 = bx * bx + by * by + 0.0 * 0.0;
+            }
+            if (with_dt) {
+                const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[g.npz]);
+                double w1, w2, w3, w4, um;
+                dt_terms(ph, u, v, 0.0, ro1, t, b2, dd, L.rkapa[g.npz], w1, w2, w3, w4, um);
+                m1 = fold_min(m1, w1); m2 = fold_min(m2, w2); m3 = fold_min(m3, w3);
+                m4 = fold_min(m4, w4); mu = fold_max(mu, um);
+            }
+        }
+    }
+    if (with_dt) reduce_dt(red, m1, m2, m3, m4, mu, sc);
+}
+
+cudaError_t launch_bcon(const Geometry& g, const Physics& ph, const Lines& L, const Boundary& b,
+                        const FieldSet& fs, Scalars* sc, int with_dt, cudaStream_t st) {
+    dim3 block(32, 8, 1);
+    dim3 grid((g.npx + 31) / 32, (g.npy + 7) / 8, 1);
+    bcon_kernel<<<grid, block, 0, st>>>(g, ph, L, b, fs, sc, with_dt);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------
+// Full-domain time-step limits of the current state (used after an upload, and after a
+// partial step, to seed the reduction the next step starts from).
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) dt_full_kernel(Geometry g, Physics ph, Lines L,
+                                                      FieldSet fs, Scalars* sc) {
+    __shared__ double red[5 * 8];
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    double m1 = 1e300, m2 = 1e300, m3 = 1e300, m4 = 1e300, mu = 0.0;
+    if (i <= g.npx && j <= g.npy) {
+        const double dxy = (L.ddy[j] < L.ddx[i]) ? L.ddy[j] : L.ddx[i];
+        for (int k = 1 + blockIdx.z; k <= g.npz; k += gridDim.z) {
+            const int64_t n = (int64_t)k * g.plane + (int64_t)j * g.pitch + i;
+            double b2 = 0.0;
+            if (ph.lmag) {
+                const double bx = fs.xin[5][n], by = fs.xin[6][n], bz = fs.xin[7][n];
+                b2 = bx * bx + by * by + bz * bz;
+            }
+            const double dd = (L.ddz[k] < dxy) ? L.ddz[k] : dxy;
+            double w1, w2, w3, w4, um;
+            dt_terms(ph, fs.xin[0][n], fs.xin[1][n], fs.xin[2][n], fs.xin[3][n], fs.xin[4][n], b2,
+                     dd, L.rkapa[k], w1, w2, w3, w4, um);
+            m1 = fold_min(m1, w1); m2 = fold_min(m2, w2); m3 = fold_min(m3, w3);
+            m4 = fold_min(m4, w4); mu = fold_max(mu, um);
+        }
+    }
+    reduce_dt(red, m1, m2, m3, m4, mu, sc);
+}
+
+cudaError_t launch_dt_full(const Geometry& g, const Physics& ph, const Lines& L,
+                           const FieldSet& fs, Scalars* sc, cudaStream_t st) {
+    dim3 block(32, 8, 1);
+    dim3 grid((g.npx + 31) / 32, (g.npy + 7) / 8, (unsigned)min(g.npz, 64));
+    dt_full_kernel<<<grid, block, 0, st>>>(g, ph, L, fs, sc);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------
+// Scalar bookkeeping: dt = sff*min(...) and umach = sqrt(max(...)) at the start of a step
+// (src/step.cpp:133-141, 224-229), and nit/timc/timt at its end (src/step.cpp:254-256).
+// ---------------------------------------------------------------------------------------
+__global__ void step_begin_kernel(Physics ph, Scalars* sc) {
+    const double w0 = order_value(sc->wmin[0]), w1 = order_value(sc->wmin[1]);
+    const double w2 = order_value(sc->wmin[2]), w3 = order_value(sc->wmin[3]);
+    double m = (w1 < w0) ? w1 : w0;
+    m = (w2 < m) ? w2 : m;
+    if (ph.lmag) m = (w3 < m) ? w3 : m;
+    sc->dt = ph.sff * m;
+    sc->umach = sqrt(order_value(sc->umax));
+    sc->wmin[0] = sc->wmin[1] = sc->wmin[2] = sc->wmin[3] = order_key(1e300);
+    sc->umax = order_key(0.0);
+}
+
+__global__ void step_end_kernel(Scalars* sc) {
+    sc->nit += 1;
+    sc->timc += sc->dt;
+    sc->timt = sc->timi + sc->timc;
+}
+
+__global__ void reset_reduction_kernel(Scalars* sc) {
+    sc->wmin[0] = sc->wmin[1] = sc->wmin[2] = sc->wmin[3] = order_key(1e300);
+    sc->umax = order_key(0.0);
+}
+
+cudaError_t launch_step_begin(const Physics& ph, Scalars* sc, cudaStream_t st) {
+    step_begin_kernel<<<1, 1, 0, st>>>(ph, sc);
+    return cudaGetLastError();
+}
+cudaError_t launch_step_end(Scalars* sc, cudaStream_t st) {
+    step_end_kernel<<<1, 1, 0, st>>>(sc);
+    return cudaGetLastError();
+}
+cudaError_t launch_reset_reduction(Scalars* sc, cudaStream_t st) {
+    reset_reduction_kernel<<<1, 1, 0, st>>>(sc);
+    return cudaGetLastError();
+}
+
+}  // namespace r3dk

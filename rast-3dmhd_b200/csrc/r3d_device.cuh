@@ -44,6 +44,9 @@ struct Lines {
     const double *plume_x, *plume_y;                          // [npx+2], [npy+2]
 };
 
+// Error codes stored in Scalars::err by kernels that abandon a bounded wait.
+enum { kErrNone = 0, kErrTmaTimeout = 1 };
+
 // Boundary set-up for the BCON kernel (src/bcon.cpp:12-141).
 struct Boundary {
     int top_mode;     // 0 const T=1, 1 const flux, 2 plume T, 3 plume flux, 4 half-domain T
@@ -56,7 +59,7 @@ struct Boundary {
 struct Scalars {
     double dt, timc, timt, timi, umach, tb;
     int nit;
-    int pad;
+    int err;  // nonzero: a kernel gave up on a bounded wait (code = kernel id)
     unsigned long long wmin[4];  // keys of min(ww1), min(ww2), min(ww3), min(vv)
     unsigned long long umax;     // key of max(ogamma*uu/tt)
     double mass, energy;         // diagnostics (r3d_gpu_totals)

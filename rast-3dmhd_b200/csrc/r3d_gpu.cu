@@ -11,6 +11,7 @@
 //  * dt, umach, nit, timc, timt live on the device; a step is 8 kernel launches with no host
 //    round trip (the reference copies three full arrays to the host per step for dt,
 //    src/gpu.cpp:790-823).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -33,6 +34,40 @@ inline void cuda_ok(cudaError_t e, const char* what) {
     if (e != cudaSuccess)
         throw Error(e == cudaErrorMemoryAllocation ? R3D_ENOMEM : R3D_ECUDA,
                     std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed).
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_fn() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        cuda_ok(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q),
+                "cudaGetDriverEntryPoint(cuTensorMapEncodeTiled)");
+        if (!f || q != cudaDriverEntryPointSuccess) throw Error(R3D_ECUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = (EncodeTiled)f;
+    }
+    return fn;
+}
+
+// 3D map over one padded field: dims (npx+2, npy+2, npz+2), box (34, 10, 1).  Reads past the
+// x/y extent of the last tiles are zero-filled by the TMA unit and never used.
+CUtensorMap field_map(void* base, int64_t nx, int64_t ny, int64_t nz, int64_t pitch, int64_t plane,
+                      cuuint32_t box_x, cuuint32_t box_y, CUtensorMapDataType type, size_t esize) {
+    CUtensorMap m;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)(pitch * esize), (cuuint64_t)(plane * esize)};
+    const cuuint32_t box[3] = {box_x, box_y, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode_fn()(&m, type, 3, base, dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(R3D_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
 }
 
 __global__ void totals_kernel(r3dk::Geometry g, r3dk::Physics ph, FieldSet fs, r3dk::Scalars* sc) {
@@ -81,6 +116,7 @@ struct r3d_gpu {
     r3dk::Boundary bnd{};
     int nfields = 5;
     double* X[2][r3dk::kMaxFields] = {};
+    r3dk::StageMaps maps[2];  // TMA maps of X[0] and X[1] (ru rv rw ro tt)
     double* Z[r3dk::kMaxFields] = {};
     double* line_buf = nullptr;
     r3dk::Scalars* dsc = nullptr;
@@ -161,7 +197,7 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
         if (g->p.lmag)
             cuda_ok(r3dk::launch_stage_mhd_fp64(s, g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage_mhd");
         else
-            cuda_ok(r3dk::launch_stage_fp64(s, g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage");
+            cuda_ok(r3dk::launch_stage_fp64(s, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage");
         tm.end(0);
         tm.begin();
         cuda_ok(r3dk::launch_bcon(g->geo, g->ph, g->lines, g->bnd, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon");
@@ -185,6 +221,9 @@ void pull_scalars(r3d_gpu* g, r3d_scalars* sc) {
     cuda_ok(cudaMemcpyAsync(g->hsc, g->dsc, sizeof(r3dk::Scalars), cudaMemcpyDeviceToHost, g->stream),
             "scalar read-back");
     cuda_ok(cudaStreamSynchronize(g->stream), "step");
+    if (g->hsc->err != r3dk::kErrNone)
+        throw Error(R3D_ECUDA, "a stage kernel abandoned a bounded TMA wait (error " +
+                                   std::to_string(g->hsc->err) + "); the state is invalid");
     g->host_timc = g->hsc->timc;
     g->host_timi = g->hsc->timi;
     if (sc) {
@@ -328,6 +367,12 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
                     cuda_ok(cudaMalloc(&g->X[b][q], nbytes), "cudaMalloc(state)");
                     g->bytes += nbytes;
                 }
+            unsigned bx = 0, by = 0;
+            r3dk::stage_fp64_box(&bx, &by);  // the box the stage kernel expects per plane
+            for (int b = 0; b < 2; ++b)
+                for (int q = 0; q < 5; ++q)
+                    g->maps[b].m[q] = field_map(g->X[b][q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
+                                                bx, by, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double));
             for (int q = 0; q < g->nfields; ++q) {
                 cuda_ok(cudaMalloc(&g->Z[q], nbytes), "cudaMalloc(accumulator)");
                 cuda_ok(cudaMemsetAsync(g->Z[q], 0, nbytes, g->stream), "cudaMemset");
@@ -356,7 +401,11 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
             b.bottom_mode = p->izcon;
             b.hh = p->hh; b.theta = p->theta; b.tp = p->tp; b.tpr = p->tp;
             b.half_nx = (int)(d.nx / 2);
-            g->kchunk = p->npz >= 256 ? 32 : 16;
+            #ifdef R3D_KCHUNK
+            g->kchunk = R3D_KCHUNK;
+#else
+            g->kchunk = p->npz >= 512 ? 64 : (p->npz >= 256 ? 32 : 16);
+#endif
             cuda_ok(cudaStreamSynchronize(g->stream), "create");
         } catch (...) {
             r3d_gpu_destroy(g);

@@ -1,6 +1,7 @@
 // r3d_kernels.h - launchers of the step kernels (host side of csrc/*.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "r3d_device.cuh"
@@ -22,9 +23,18 @@ struct FieldSet32 {
     float* z[5];
 };
 
+// TMA descriptors of the five state fields read by a stage (ru rv rw ro tt): a 3D map over
+// (x, y, z) = (npx+2, npy+2, npz+2) doubles with the padded row pitch, box 34 x 10 x 1.
+struct StageMaps {
+    CUtensorMap m[5];
+};
+
 size_t stage_fp64_smem();
-cudaError_t launch_stage_fp64(int stage, const Geometry& g, const Physics& ph, const Lines& L,
-                              const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st);
+// TMA box (x, y) of one field plane that the FP64 stage kernel was compiled for.
+void stage_fp64_box(unsigned* bx, unsigned* by);
+cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
+                              const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
+                              int kchunk, cudaStream_t st);
 cudaError_t launch_stage_mhd_fp64(int stage, const Geometry& g, const Physics& ph,
                                   const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk,
                                   cudaStream_t st);
