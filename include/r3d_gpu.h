@@ -128,6 +128,23 @@ int r3d_gpu_run_timed(r3d_gpu* g, int nsteps, r3d_scalars* sc, r3d_timing* tm);
  * the device (mass = sum rho, energy = sum (rho*T*cv + 0.5*(ru^2+rv^2+rw^2)/rho)). */
 int r3d_gpu_totals(r3d_gpu* g, double* mass, double* energy);
 
+/* ---- allocation-free time-step limits (no counterpart in the reference) ----
+ * For callers that cannot call cudaMalloc (for example a program that reserves the GPU's memory
+ * in its own pool up front, or a time loop that must not pay the device synchronisation that
+ * cudaMalloc/cudaFree may imply): computes {dt, umach} of a state the caller already holds in
+ * device memory, as the next step would (src/step.cpp:122-229), using a fixed file-scope device
+ * array for its partial results instead of allocated scratch.
+ *   fields: 8 device pointers ru rv rw ro tt bx by bz (bx..bz only read when lmag), each the
+ *           global (npx+2)(npy+2)(npz+2) array in the layout above;
+ *   lines:  4 device pointers ddx[npx+2], ddy[npy+2], ddz[npz+2], rkapa[npz+2];
+ *   out:    device pointer to 2 doubles, receives dt and umach;
+ *   stream: cudaStream_t to launch on (NULL = legacy default stream); runs on device p->gpu_id.
+ * Limit: ceil(npx/32)*ceil(npy/8) <= 65536 column tiles, else R3D_EINVAL.  Calls share the
+ * array, so calls that overlap on the GPU race; the first call on a device looks up the
+ * array's address and should come before any stream capture.  Allocates no device memory. */
+int r3d_dt_limits_noalloc(const r3d_params* p, const double* const* fields,
+                          const double* const* lines, double* out, void* stream);
+
 /* Message of the calling thread's last failed call ("" if none). */
 const char* r3d_last_error(void);
 /* Library version string. */
