@@ -64,6 +64,7 @@ class Oracle:
             lib.ora_init.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.ora_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.ora_fluxes.argtypes = [ctypes.c_void_p]
+            lib.ora_communicate.argtypes = [ctypes.c_void_p]
             lib.ora_field.restype = ctypes.POINTER(ctypes.c_double)
             lib.ora_field.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.ora_line.restype = ctypes.POINTER(ctypes.c_double)
@@ -106,6 +107,9 @@ class Oracle:
 
     def fluxes(self):
         self._check(self.lib().ora_fluxes(self.h))
+
+    def communicate(self):
+        self.lib().ora_communicate(self.h)
 
     def field(self, name: str) -> np.ndarray:
         """A live view of a 3D field, shape (NZ, NY, NX)."""

@@ -174,8 +174,7 @@ ora_sim* ora_create(int argc, const char** argv) {
     params_default(&s->p);
     if (parse(argc, argv, &s->p) != 0) { free(s); return NULL; }
     const ora_params* p = &s->p;
-    if (p->ix != 2 || p->iy != 2 || p->ilap != 2) { set_err("ix/iy/ilap must be 2"); free(s); return NULL; }
-    if (p->npx < 3 || p->npy < 3 || p->npz < 4) { set_err("grid too small"); free(s); return NULL; }
+    if (p->npx < 1 || p->npy < 1 || p->npz < 1) { set_err("grid extents must be positive"); free(s); return NULL; }
     s->NX = p->npx + 2; s->NY = p->npy + 2; s->NZ = p->npz + 2;
     s->N = (long)s->NX * s->NY * s->NZ;
     for (int q = 0; q < ORA_NFIELDS; ++q) s->f[q] = (double*)calloc(s->N, sizeof(double));
@@ -505,6 +504,8 @@ static void communicate(ora_sim* s) {
 /* src/static_ic.cpp:24-161 + src/main.cpp:148-154 on the global domain. */
 int ora_init(ora_sim* s, int seed) {
     const ora_params* p = &s->p;
+    if (p->ix != 2 || p->iy != 2 || p->ilap != 2) { set_err("ix/iy/ilap must be 2"); return -1; }
+    if (p->npx < 3 || p->npy < 3 || p->npz < 4) { set_err("grid too small"); return -1; }
     if (p->nstart != 0) { set_err("restart (nstart != 0) is not supported"); return -1; }
     if (p->lshr || p->lrem) { set_err("LSHR/LREM not supported"); return -1; }
     if (p->lmag && p->ntube != 0) { set_err("TUBE models not supported"); return -1; }
@@ -836,6 +837,7 @@ static void fluxes(ora_sim* s) {
 }
 
 int ora_fluxes(ora_sim* s) { fluxes(s); return 0; }
+void ora_communicate(ora_sim* s) { communicate(s); }
 
 /* ------------------------------------------------------------------- BCON --------- */
 /* src/bcon.cpp:12-141 for the global top (k=1) and bottom (k=npz) planes. */

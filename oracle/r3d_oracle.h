@@ -40,6 +40,8 @@ int ora_init(ora_sim* s, int seed);
 int ora_step(ora_sim* s, int nstages);
 /* One FLUXES evaluation on the current state (overwrites RO with 1/RO like the reference). */
 int ora_fluxes(ora_sim* s);
+/* The halo exchange of the primaries (+B) on the global domain (periodic x/y copies). */
+void ora_communicate(ora_sim* s);
 
 double* ora_field(ora_sim* s, int id);
 double* ora_line(ora_sim* s, int id);
