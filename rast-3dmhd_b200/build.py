@@ -17,7 +17,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "host"), "-I", os.path.join(PKG, "csrc")]
 HOST_SRCS = ["host/params.cpp", "host/setup.cpp"]
-CU_SRCS = ["csrc/step_fp64.cu", "csrc/bcon.cu", "csrc/step_mhd_fp64.cu", "csrc/step_fp32.cu", "csrc/r3d_gpu.cu", "csrc/dt_noalloc.cu"]
+CU_SRCS = ["csrc/step_fp64.cu", "csrc/bcon.cu", "csrc/step_fp32.cu", "csrc/r3d_gpu.cu", "csrc/dt_noalloc.cu"]
 LIB = os.path.join(PKG, "lib", "librast3d_b200.so")
 BIN = os.path.join(PKG, "bin", "r3d_b200")
 

@@ -22,7 +22,7 @@ struct Geometry {
 };
 
 struct Physics {
-    double hx, h2x, hy, hz;
+    double hx, h2x, hy, hz, h2y, h2z;
     double c13, c23, c43, ore, ocv, grav;
     double tdiff;    // ocv/repr                     (src/fluxes.cpp:247)
     double theat;    // ocv*ore                      (src/fluxes.cpp:344)
@@ -30,6 +30,7 @@ struct Physics {
     double t13;      // c13*ore                      (src/fluxes.cpp:362)
     double omx, omz;
     double gamma, ogamma, re, repr, cv, rm, obeta, orm, sff;
+    double tmag;     // obeta*orm*ocv                (3dmhdsub.f:2308)
     double gam[3], zeta[3];
     int lrot, lmag;
     int kappa_const;  // rkapa == 1 and dkapa == 0 on every plane (exact shortcut)
@@ -38,7 +39,7 @@ struct Physics {
 // 1D metric tables (device pointers).
 struct Lines {
     const double *dxxdx, *d2xxdx2, *ddx;                      // [npx+2]
-    const double *dyydy, *tmpy, *tmpy1, *tmpy2, *ddy;         // [npy+2]
+    const double *dyydy, *d2yydy2, *tmpy, *tmpy1, *tmpy2, *ddy;  // [npy+2]
     const double *dzzdz, *d2zzdz2, *tmpz, *tmpz1, *tmpz2;     // [npz+2]
     const double *ddz, *rkapa, *dkapa;                        // [npz+2]
     const double *plume_x, *plume_y;                          // [npx+2], [npy+2]

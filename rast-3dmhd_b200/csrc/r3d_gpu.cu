@@ -194,10 +194,7 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
     for (int s = 0; s < nstages; ++s) {
         FieldSet fs = fieldset(g);
         tm.begin();
-        if (g->p.lmag)
-            cuda_ok(r3dk::launch_stage_mhd_fp64(s, g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage_mhd");
-        else
-            cuda_ok(r3dk::launch_stage_fp64(s, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage");
+        cuda_ok(r3dk::launch_stage_fp64(s, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage");
         tm.end(0);
         tm.begin();
         cuda_ok(r3dk::launch_bcon(g->geo, g->ph, g->lines, g->bnd, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon");
@@ -276,7 +273,8 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
     // host tables (products keep the reference association)
     std::vector<double> dxxdx(st->dxxdx, st->dxxdx + NX), d2xxdx2(st->d2xxdx2, st->d2xxdx2 + NX),
         ddx(st->ddx, st->ddx + NX);
-    std::vector<double> dyydy(st->dyydy, st->dyydy + NY), ddy(st->ddy, st->ddy + NY);
+    std::vector<double> dyydy(st->dyydy, st->dyydy + NY), ddy(st->ddy, st->ddy + NY),
+        d2yydy2(st->d2yydy2, st->d2yydy2 + NY);
     std::vector<double> tmpy(NY), tmpy1(NY), tmpy2(NY);
     for (int64_t j = 0; j < NY; ++j) {
         tmpy[j] = d.hy * st->dyydy[j];                       // src/fluxes.cpp:90
@@ -305,7 +303,7 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
     std::vector<const std::vector<double>*> tabs = {&dxxdx, &d2xxdx2, &ddx,  &dyydy, &tmpy,
                                                     &tmpy1, &tmpy2,   &ddy,  &dzzdz, &d2zzdz2,
                                                     &tmpz,  &tmpz1,   &tmpz2, &ddz,  &rkapa,
-                                                    &dkapa, &px,      &py};
+                                                    &dkapa, &px,      &py,   &d2yydy2};
     size_t total = 0;
     for (auto* t : tabs) total += (t->size() + 15) / 16 * 16;
     if (!g->line_buf) {
@@ -327,6 +325,7 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
     L.dyydy = dev[3]; L.tmpy = dev[4]; L.tmpy1 = dev[5]; L.tmpy2 = dev[6]; L.ddy = dev[7];
     L.dzzdz = dev[8]; L.d2zzdz2 = dev[9]; L.tmpz = dev[10]; L.tmpz1 = dev[11]; L.tmpz2 = dev[12];
     L.ddz = dev[13]; L.rkapa = dev[14]; L.dkapa = dev[15]; L.plume_x = dev[16]; L.plume_y = dev[17];
+    L.d2yydy2 = dev[18];
     bool kc = true;
     for (int64_t k = 1; k <= NZ - 2; ++k) kc = kc && rkapa[k] == 1.0 && dkapa[k] == 0.0;
     g->ph.kappa_const = kc ? 1 : 0;
@@ -370,7 +369,7 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
             unsigned bx = 0, by = 0;
             r3dk::stage_fp64_box(&bx, &by);  // the box the stage kernel expects per plane
             for (int b = 0; b < 2; ++b)
-                for (int q = 0; q < 5; ++q)
+                for (int q = 0; q < g->nfields; ++q)
                     g->maps[b].m[q] = field_map(g->X[b][q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
                                                 bx, by, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double));
             for (int q = 0; q < g->nfields; ++q) {
@@ -381,7 +380,8 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
             cuda_ok(cudaMalloc(&g->dsc, sizeof(r3dk::Scalars)), "cudaMalloc(scalars)");
             cuda_ok(cudaMallocHost(&g->hsc, sizeof(r3dk::Scalars)), "cudaMallocHost");
             r3dk::Physics& ph = g->ph;
-            ph.hx = d.hx; ph.h2x = d.h2x; ph.hy = d.hy; ph.hz = d.hz;
+            ph.hx = d.hx; ph.h2x = d.h2x; ph.hy = d.hy; ph.hz = d.hz; ph.h2y = d.h2y; ph.h2z = d.h2z;
+            ph.tmag = d.obeta * d.orm * d.ocv;  // 3dmhdsub.f:2308
             ph.c13 = d.c13; ph.c23 = d.c23; ph.c43 = d.c43; ph.ore = d.ore; ph.ocv = d.ocv;
             ph.grav = p->grav;
             ph.tdiff = d.ocv / d.repr;

@@ -23,10 +23,11 @@ struct FieldSet32 {
     float* z[5];
 };
 
-// TMA descriptors of the five state fields read by a stage (ru rv rw ro tt): a 3D map over
-// (x, y, z) = (npx+2, npy+2, npz+2) doubles with the padded row pitch, box 34 x 10 x 1.
+// TMA descriptors of the state fields read by a stage (ru rv rw ro tt, + bx by bz with MHD):
+// a 3D map over (x, y, z) = (npx+2, npy+2, npz+2) doubles with the padded row pitch, one
+// (34, TY+2, 1) box per plane.
 struct StageMaps {
-    CUtensorMap m[5];
+    CUtensorMap m[kMaxFields];
 };
 
 size_t stage_fp64_smem();
@@ -35,9 +36,6 @@ void stage_fp64_box(unsigned* bx, unsigned* by);
 cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
                               const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
                               int kchunk, cudaStream_t st);
-cudaError_t launch_stage_mhd_fp64(int stage, const Geometry& g, const Physics& ph,
-                                  const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk,
-                                  cudaStream_t st);
 cudaError_t launch_bcon(const Geometry& g, const Physics& ph, const Lines& L, const Boundary& b,
                         const FieldSet& fs, Scalars* sc, int with_dt, cudaStream_t st);
 cudaError_t launch_dt_full(const Geometry& g, const Physics& ph, const Lines& L,

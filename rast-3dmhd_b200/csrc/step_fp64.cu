@@ -1,28 +1,33 @@
-// step_fp64.cu - the fused FP64 RK3 stage kernel (hydro).
+// step_fp64.cu - the fused FP64 RK3 stage kernel (hydro and MHD).
 //
 // One launch per Wray stage computes, for every interior cell, the complete FLUXES right-hand
-// side of src/fluxes.cpp:87-514 and applies the stage update of src/step.cpp:53-110 in its
-// epilogue:
+// side of src/fluxes.cpp:87-533 (with MHD, also the LMAG branch of
+// golden/fortran/3dmhdsub.f:2146-2650: Lorentz force, ohmic heating, induction and magnetic
+// diffusion) and applies the stage update of src/step.cpp:53-110 (3dmhdsub.f:957-1177 for B)
+// in its epilogue:
 //     X' = Z + gam_s*dt*F            (Z = X at stage 1; the save_state copy is never made)
 //     Z' = X' + zeta_{s+1}*dt*F      (stages 1 and 2; the reference's next mix_state)
-// F is never stored.  The reference evaluates FLUXES as ~40 full-array sweeps with WW1..WW3
-// temporaries; here every temporary is re-evaluated per cell with the literal expression the
-// reference uses for it, and each accumulator (FU, FV, FW, FR, FT) receives its terms in the
-// reference's order, so with FMA contraction off (-fmad=false) the result is bit-identical.
+// F is never stored.  The reference evaluates FLUXES as ~40 full-array sweeps (~80 with LMAG)
+// with WW1..WW3 and RU..TT as temporaries; here every temporary is re-evaluated per cell with
+// the literal expression the reference uses for it, and each accumulator (FU, FV, FW, FR, FT,
+// and the B fluxes WW1..WW3) receives its terms in the reference's order, so with FMA
+// contraction off (-fmad=false) the result is bit-identical.
 //
-// Pipeline: a CTA owns a 32x8 column tile and marches down a chunk of z planes.  Thread 0
-// streams the five state fields of each plane, with a one-cell x/y halo, into a 4-slot ring
-// by TMA (one 34x10x1 box per field, completion on a per-slot mbarrier), two planes ahead of
+// Pipeline: a CTA owns a 32 x TY column tile and marches down a chunk of z planes.  Thread 0
+// streams the state fields of each plane, with a one-cell x/y halo, into a 4-slot ring by TMA
+// (one (34, TY+2, 1) box per field, completion on a per-slot mbarrier), two planes ahead of
 // the plane being computed.  Each loaded cell is then turned once into 1/rho, u, v, w and
 // P = rho*T (src/fluxes.cpp:131-166) in a second 4-slot ring, so a single __syncthreads per
 // plane orders everything: the plane k+1 derivation, the TMA refill of the slot of plane k-2,
 // and the compute of plane k, which reads the 19-point stencil (the twelve edge neighbours of
 // u, v, w come from the cross terms :367-374, :449-456, :496-498) from shared memory.
-// Planes k = 1 and k = npz carry only the continuity flux: their momenta and T are rewritten
-// by BCON (src/bcon.cpp:27-140) and the one-sided dRW/dz there (src/fluxes.cpp:106-117) reads
-// two planes inward.  Ghost columns of X' are written by the owning thread (the periodic
-// exchange of src/communicate.cpp:70-168).  The third stage also evaluates, on the finished
-// state, the per-cell time-step limits of the next step (src/step.cpp:122-229).
+// Planes k = 1 and k = npz carry only the continuity flux and, with MHD, the Bx/By fluxes:
+// their momenta, T and Bz are rewritten by BCON (src/bcon.cpp:27-140); the one-sided
+// z-derivatives there (src/fluxes.cpp:106-117, 3dmhdsub.f:2245-2259, 2468-2487, 2577-2596)
+// reach up to three planes inward and read those planes from global memory.  Ghost columns
+// of X' are written by the owning thread (the periodic exchange of src/communicate.cpp:
+// 70-168).  The third stage also evaluates, on the finished state, the per-cell time-step
+// limits of the next step (src/step.cpp:122-229).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -30,42 +35,49 @@
 #include "stage_common.cuh"
 #include "tma.cuh"
 
-namespace r3dk {
-
 #ifndef R3D_STAGE_TY
 #define R3D_STAGE_TY 8
 #endif
 
+namespace r3dk {
+
 namespace {
 constexpr int TX = 32, TY = R3D_STAGE_TY, NT = TX * TY;
-constexpr int kMinBlocks = (NT <= 256) ? 2 : 1;
-constexpr int SX = TX + 2, SY = TY + 2, SN = SX * SY;  // 340 cells per halo tile
-constexpr int RAWF = (SN + 15) / 16 * 16;   // doubles per raw field box, 128 B multiple
-enum { R_RU, R_RV, R_RW, R_RO, R_TT, R_NF };
+constexpr int SX = TX + 2, SY = TY + 2, SN = SX * SY;  // cells per halo tile
+constexpr int RAWF = (SN + 15) / 16 * 16;  // doubles per raw field box, 128 B multiple
+enum { R_RU, R_RV, R_RW, R_RO, R_TT, R_BX, R_BY, R_BZ };
 enum { D_U, D_V, D_W, D_P, D_RI, D_NF };
 constexpr int NRAW = 4, NDER = 4;
-constexpr int RAW_SLOT = R_NF * RAWF;      // doubles
-constexpr int DER_SLOT = D_NF * SN;        // doubles
-constexpr size_t kRawBytes = (size_t)NRAW * RAW_SLOT * sizeof(double);
-constexpr size_t kDerBytes = (size_t)NDER * DER_SLOT * sizeof(double);
-constexpr uint32_t kPlaneTx = R_NF * SN * sizeof(double);  // TMA bytes per plane
-constexpr size_t kSmem = kRawBytes + kDerBytes + 64;
+
+template <bool MHD>
+struct Shape {
+    static constexpr int nf = MHD ? 8 : 5;                 // raw fields per plane
+    static constexpr int raw_slot = nf * RAWF;             // doubles
+    static constexpr int der_slot = D_NF * SN;             // doubles
+    static constexpr size_t raw_bytes = (size_t)NRAW * raw_slot * sizeof(double);
+    static constexpr size_t der_bytes = (size_t)NDER * der_slot * sizeof(double);
+    static constexpr uint32_t plane_tx = nf * SN * sizeof(double);  // TMA bytes per plane
+    static constexpr size_t smem = raw_bytes + der_bytes + 64;
+    static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && NT <= 256) ? 2 : 1;
+};
 }  // namespace
 
-size_t stage_fp64_smem() { return kSmem; }
+size_t stage_fp64_smem() { return Shape<false>::smem; }
 void stage_fp64_box(unsigned* bx, unsigned* by) {
     *bx = SX;
     *by = SY;
 }
 
-template <int STAGE, bool KC>
-__global__ void __launch_bounds__(NT, kMinBlocks)
-    stage_hydro_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
-                     FieldSet fs, Scalars* sc, int kchunk) {
+template <int STAGE, bool KC, bool MHD>
+__global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
+    stage_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
+               FieldSet fs, Scalars* sc, int kchunk) {
+    using S = Shape<MHD>;
+    constexpr int NF = S::nf;
     extern __shared__ __align__(128) unsigned char smem[];
     double* raw = reinterpret_cast<double*>(smem);
-    double* der = reinterpret_cast<double*>(smem + kRawBytes);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kRawBytes + kDerBytes);
+    double* der = reinterpret_cast<double*>(smem + S::raw_bytes);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::raw_bytes + S::der_bytes);
     __shared__ int s_abort;
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -82,17 +94,17 @@ __global__ void __launch_bounds__(NT, kMinBlocks)
         last_issued = p;
         const int q = p - (kb - 1);
         uint64_t* bar = &bars[q % NRAW];
-        double* dst = raw + (q % NRAW) * RAW_SLOT;
-        mbar_expect_tx(bar, kPlaneTx);
+        double* dst = raw + (q % NRAW) * S::raw_slot;
+        mbar_expect_tx(bar, S::plane_tx);
 #pragma unroll
-        for (int f = 0; f < R_NF; ++f) tma_load_3d(dst + f * RAWF, &maps.m[f], bar, i0 - 1, j0 - 1, p);
+        for (int f = 0; f < NF; ++f) tma_load_3d(dst + f * RAWF, &maps.m[f], bar, i0 - 1, j0 - 1, p);
     };
     auto derive = [&](int p) -> bool {
         const int q = p - (kb - 1);
         if (!mbar_wait(&bars[q % NRAW], (q / NRAW) & 1)) return false;
         last_waited = p;
-        const double* r = raw + (q % NRAW) * RAW_SLOT;
-        double* d = der + (q % NDER) * DER_SLOT;
+        const double* r = raw + (q % NRAW) * S::raw_slot;
+        double* d = der + (q % NDER) * S::der_slot;
         for (int c = tid; c < SN; c += NT) {
             const double ro = r[R_RO * RAWF + c];
             const double ri = __drcp_rn(ro);  // == 1.0/ro, src/fluxes.cpp:137
@@ -132,11 +144,13 @@ __global__ void __launch_bounds__(NT, kMinBlocks)
     const double dyj = L.dyydy[ja], tmpy = L.tmpy[ja], tmpy1 = L.tmpy1[ja], tmpy2 = L.tmpy2[ja];
 
     // RK accumulator Z of the thread's own cell, loaded one plane ahead (registers)
-    double zn[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double zn[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) zn[f] = 0.0;
     const int64_t col = (int64_t)ja * g.pitch + ia;
     if (STAGE > 0 && active) {
 #pragma unroll
-        for (int f = 0; f < 5; ++f) zn[f] = fs.z[f][(int64_t)kb * g.plane + col];
+        for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][(int64_t)kb * g.plane + col];
     }
 
     for (int k = kb; k <= ke; ++k) {
@@ -148,51 +162,66 @@ __global__ void __launch_bounds__(NT, kMinBlocks)
             fence_proxy_async();
             issue(k + 2);
         }
-        double zq[5];
+        double zq[NF];
 #pragma unroll
-        for (int f = 0; f < 5; ++f) zq[f] = zn[f];
+        for (int f = 0; f < NF; ++f) zq[f] = zn[f];
         if (STAGE > 0 && active && k < ke) {
 #pragma unroll
-            for (int f = 0; f < 5; ++f) zn[f] = fs.z[f][(int64_t)(k + 1) * g.plane + col];
+            for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][(int64_t)(k + 1) * g.plane + col];
         }
         if (active) {
             const int64_t nc = (int64_t)k * g.plane + col;
-            const double* rm = raw + ((q + NRAW - 1) % NRAW) * RAW_SLOT;
-            const double* r0 = raw + (q % NRAW) * RAW_SLOT;
-            const double* rp = raw + ((q + 1) % NRAW) * RAW_SLOT;
-            const double* dm = der + ((q + NDER - 1) % NDER) * DER_SLOT;
-            const double* d0 = der + (q % NDER) * DER_SLOT;
-            const double* dp = der + ((q + 1) % NDER) * DER_SLOT;
+            const double* rm = raw + ((q + NRAW - 1) % NRAW) * S::raw_slot;
+            const double* r0 = raw + (q % NRAW) * S::raw_slot;
+            const double* rp = raw + ((q + 1) % NRAW) * S::raw_slot;
+            const double* dm = der + ((q + NDER - 1) % NDER) * S::der_slot;
+            const double* d0 = der + (q % NDER) * S::der_slot;
+            const double* dp = der + ((q + 1) % NDER) * S::der_slot;
 #define RW_(P, F, DX, DY) P[(F)*RAWF + s0 + (DY)*SX + (DX)]
 #define DV_(P, F, DX, DY) P[(F)*SN + s0 + (DY)*SX + (DX)]
             const double tmpz = L.tmpz[k];
+            const bool edge = (k == 1) || (k == g.npz);
 
             // ---- continuity, src/fluxes.cpp:87-121 ----
             double fr = (RW_(r0, R_RU, -1, 0) - RW_(r0, R_RU, 1, 0)) * hx * dx1;
             fr -= (RW_(r0, R_RV, 0, 1) - RW_(r0, R_RV, 0, -1)) * tmpy;
             double dwz;
             if (k == 1)
-                dwz = (4.0 * RW_(rp, R_RW, 0, 0) - fs.xin[2][nc + 2 * g.plane]) * tmpz;
+                dwz = (4.0 * RW_(rp, R_RW, 0, 0) - fs.xin[R_RW][nc + 2 * g.plane]) * tmpz;
             else if (k == g.npz)
-                dwz = (fs.xin[2][nc - 2 * g.plane] - 4.0 * RW_(rm, R_RW, 0, 0)) * tmpz;
+                dwz = (fs.xin[R_RW][nc - 2 * g.plane] - 4.0 * RW_(rm, R_RW, 0, 0)) * tmpz;
             else
                 dwz = (RW_(rp, R_RW, 0, 0) - RW_(rm, R_RW, 0, 0)) * tmpz;
             fr -= dwz;
 
             double fu = 0.0, fv = 0.0, fw = 0.0, ft = 0.0;
-            if (k != 1 && k != g.npz) {
-                const double dzk = L.dzzdz[k], tmpz1 = L.tmpz1[k], tmpz2 = L.tmpz2[k];
-                const double U0 = DV_(d0, D_U, 0, 0), V0 = DV_(d0, D_V, 0, 0), W0 = DV_(d0, D_W, 0, 0);
-                const double T0 = RW_(r0, R_TT, 0, 0), ri = DV_(d0, D_RI, 0, 0);
-                const double Uxp = DV_(d0, D_U, 1, 0), Uxm = DV_(d0, D_U, -1, 0);
-                const double Uyp = DV_(d0, D_U, 0, 1), Uym = DV_(d0, D_U, 0, -1);
-                const double Uzp = DV_(dp, D_U, 0, 0), Uzm = DV_(dm, D_U, 0, 0);
-                const double Vxp = DV_(d0, D_V, 1, 0), Vxm = DV_(d0, D_V, -1, 0);
-                const double Vyp = DV_(d0, D_V, 0, 1), Vym = DV_(d0, D_V, 0, -1);
-                const double Vzp = DV_(dp, D_V, 0, 0), Vzm = DV_(dm, D_V, 0, 0);
-                const double Wxp = DV_(d0, D_W, 1, 0), Wxm = DV_(d0, D_W, -1, 0);
-                const double Wyp = DV_(d0, D_W, 0, 1), Wym = DV_(d0, D_W, 0, -1);
-                const double Wzp = DV_(dp, D_W, 0, 0), Wzm = DV_(dm, D_W, 0, 0);
+            double b1 = 0.0, b2f = 0.0, b3 = 0.0;  // B fluxes WW1..WW3 (MHD)
+            const double dzk = L.dzzdz[k];
+            const double U0 = DV_(d0, D_U, 0, 0), V0 = DV_(d0, D_V, 0, 0), W0 = DV_(d0, D_W, 0, 0);
+            const double ri = DV_(d0, D_RI, 0, 0);
+            const double Uxp = DV_(d0, D_U, 1, 0), Uxm = DV_(d0, D_U, -1, 0);
+            const double Uyp = DV_(d0, D_U, 0, 1), Uym = DV_(d0, D_U, 0, -1);
+            const double Uzp = DV_(dp, D_U, 0, 0), Uzm = DV_(dm, D_U, 0, 0);
+            const double Vxp = DV_(d0, D_V, 1, 0), Vxm = DV_(d0, D_V, -1, 0);
+            const double Vyp = DV_(d0, D_V, 0, 1), Vym = DV_(d0, D_V, 0, -1);
+            const double Vzp = DV_(dp, D_V, 0, 0), Vzm = DV_(dm, D_V, 0, 0);
+            const double Wxp = DV_(d0, D_W, 1, 0), Wxm = DV_(d0, D_W, -1, 0);
+            const double Wyp = DV_(d0, D_W, 0, 1), Wym = DV_(d0, D_W, 0, -1);
+            const double Wzp = DV_(dp, D_W, 0, 0), Wzm = DV_(dm, D_W, 0, 0);
+            // velocity gradients, the reference's WW1..WW3 / RU..RW temporaries
+            const double ux = (Uxp - Uxm) * hx * dx1;  // src/fluxes.cpp:331,416; 3dmhdsub.f:2151
+            const double vx = (Vxp - Vxm) * hx * dx1;  // :336; 3dmhdsub.f:2157
+            const double wx = (Wxp - Wxm) * hx * dx1;  // :341,505; 3dmhdsub.f:2163
+            const double uy = (Uyp - Uym) * hy * dyj;  // :382; 3dmhdsub.f:2181
+            const double vy = (Vyp - Vym) * hy * dyj;  // :397; 3dmhdsub.f:2187
+            const double wy = (Wyp - Wym) * hy * dyj;  // :476; 3dmhdsub.f:2193
+            const double uz = (Uzp - Uzm) * hz * dzk;  // :464; 3dmhdsub.f:2211
+            const double vz = (Vzp - Vzm) * hz * dzk;  // :469; 3dmhdsub.f:2217
+            const double wz = (Wzp - Wzm) * hz * dzk;  // :423; 3dmhdsub.f:2223
+
+            if (!edge) {
+                const double tmpz1 = L.tmpz1[k], tmpz2 = L.tmpz2[k];
+                const double T0 = RW_(r0, R_TT, 0, 0);
 
                 // ---- buoyancy and pressure, src/fluxes.cpp:126-152 ----
                 fw = ph.grav * RW_(r0, R_RO, 0, 0);
@@ -246,15 +275,6 @@ __global__ void __launch_bounds__(NT, kMinBlocks)
                              c43 * ((Wzp - Wzm) * tmpz1 + (Wzp - 2.0 * W0 + Wzm) * tmpz2));
 
                 // ---- viscous heating, p dV and cross terms, src/fluxes.cpp:327-514 ----
-                const double ux = (Uxp - Uxm) * hx * dx1;  // WW1 = dU/dx (:331, :416)
-                const double vx = (Vxp - Vxm) * hx * dx1;  // WW2 = dV/dx (:336)
-                const double wx = (Wxp - Wxm) * hx * dx1;  // WW3 = dW/dx (:341, :505)
-                const double uy = (Uyp - Uym) * hy * dyj;  // :382
-                const double vy = (Vyp - Vym) * hy * dyj;  // :397
-                const double wy = (Wyp - Wym) * hy * dyj;  // :476
-                const double uz = (Uzp - Uzm) * hz * dzk;  // :464
-                const double vz = (Vzp - Vzm) * hz * dzk;  // :469
-                const double wz = (Wzp - Wzm) * hz * dzk;  // :423
                 const double th = ph.theat, th43 = ph.theat43, t13 = ph.t13, ocv = ph.ocv;
                 ft += (c43 * ux * ux + vx * vx + wx * wx) * ri * th;  // :349
                 ft -= ocv * ux * T0;                                   // :357
@@ -294,25 +314,138 @@ __global__ void __launch_bounds__(NT, kMinBlocks)
                 }
             }
 
-            // ---- stage update, src/step.cpp:53-110 ----
-            const double F[5] = {fu, fv, fw, fr, ft};
+            if (MHD) {
+                // ---- magnetic terms, golden/fortran/3dmhdsub.f:2146-2650 (LMAG branch) ----
+                // At k = 1 / npz the momenta, T and Bz are rewritten by BCON afterwards; the
+                // Lorentz/ohmic contributions there are computed and discarded like the rest.
+                const double h2y = ph.h2y, h2z = ph.h2z, d2y = L.d2yydy2[ja], d2z = L.d2zzdz2[k];
+                const double ob = ph.obeta, orm = ph.orm, tmag = ph.tmag;
+                const double BX0 = RW_(r0, R_BX, 0, 0), BY0 = RW_(r0, R_BY, 0, 0), BZ0 = RW_(r0, R_BZ, 0, 0);
+                const double BXxp = RW_(r0, R_BX, 1, 0), BXxm = RW_(r0, R_BX, -1, 0);
+                const double BXyp = RW_(r0, R_BX, 0, 1), BXym = RW_(r0, R_BX, 0, -1);
+                const double BXzp = RW_(rp, R_BX, 0, 0), BXzm = RW_(rm, R_BX, 0, 0);
+                const double BYxp = RW_(r0, R_BY, 1, 0), BYxm = RW_(r0, R_BY, -1, 0);
+                const double BYyp = RW_(r0, R_BY, 0, 1), BYym = RW_(r0, R_BY, 0, -1);
+                const double BYzp = RW_(rp, R_BY, 0, 0), BYzm = RW_(rm, R_BY, 0, 0);
+                const double BZxp = RW_(r0, R_BZ, 1, 0), BZxm = RW_(r0, R_BZ, -1, 0);
+                const double BZyp = RW_(r0, R_BZ, 0, 1), BZym = RW_(r0, R_BZ, 0, -1);
+                const double BZzp = RW_(rp, R_BZ, 0, 0), BZzm = RW_(rm, R_BZ, 0, 0);
+                // dW/dz with the one-sided forms at the top and bottom planes (2245-2259)
+                double wzb = wz;
+                if (k == 1) {
+                    const int64_t n2 = nc + 2 * g.plane;
+                    const double w2 = fs.xin[R_RW][n2] * __drcp_rn(fs.xin[R_RO][n2]);
+                    wzb = (4.0 * Wzp - w2) * hz * dzk;
+                } else if (k == g.npz) {
+                    const int64_t n2 = nc - 2 * g.plane;
+                    const double w2 = fs.xin[R_RW][n2] * __drcp_rn(fs.xin[R_RO][n2]);
+                    wzb = (w2 - 4.0 * Wzm) * hz * dzk;
+                }
+                b2f = BX0 * vx - BY0 * ux;                 // 1030
+                b3 = BX0 * wx - BZ0 * ux;                  // 1040
+                b1 = BY0 * uy - BX0 * vy;                  // 1080
+                b3 = b3 + BY0 * wy - BZ0 * vy;             // 1090
+                b1 = b1 + BZ0 * uz - BX0 * wzb;            // 1130
+                b2f = b2f + BZ0 * vz - BY0 * wzb;          // 1140
+                const double bxx = (BXxp - BXxm) * hx * dx1;   // 1150
+                const double byx = (BYxp - BYxm) * hx * dx1;   // 1160
+                const double bzx = (BZxp - BZxm) * hx * dx1;   // 1170
+                const double bxy = (BXyp - BXym) * hy * dyj;   // 1180
+                fu = fu + ob * BY0 * (bxy - byx) - ob * BZ0 * bzx;  // 1190
+                fv = fv + ob * BX0 * (byx - bxy);                   // 1200
+                fw = fw + ob * BX0 * bzx;                           // 1210
+                ft = ft + (bxy * bxy + byx * byx + bzx * bzx - 2.0 * byx * bxy) * ri * tmag;  // 1220
+                b1 = b1 - U0 * bxx - V0 * bxy;             // 1230
+                b2f = b2f - U0 * byx;                      // 1240
+                b3 = b3 - U0 * bzx;                        // 1250
+                const double d2bxx = (BXxp - BXxm) * hx * d2x + (BXxp - 2.0 * BX0 + BXxm) * h2x * dx1 * dx1;  // 1260
+                const double d2byx = (BYxp - BYxm) * hx * d2x + (BYxp - 2.0 * BY0 + BYxm) * h2x * dx1 * dx1;  // 1265
+                const double d2bxy = (BXyp - BXym) * hy * d2y + (BXyp - 2.0 * BX0 + BXym) * h2y * dyj * dyj;  // 1270
+                b1 = b1 + orm * (d2bxx + d2bxy);           // 1280
+                b2f = b2f + orm * d2byx;                   // 1290
+                const double d2bzx = (BZxp - BZxm) * hx * d2x + (BZxp - 2.0 * BZ0 + BZxm) * h2x * dx1 * dx1;  // 1300
+                b3 = b3 + orm * d2bzx;                     // 1310
+                const double bxz = (BXzp - BXzm) * hz * dzk;   // 1320
+                const double byy = (BYyp - BYym) * hy * dyj;   // 1330
+                fu = fu + ob * BZ0 * bxz;                  // 1340
+                fw = fw - ob * BX0 * bxz;                  // 1350
+                ft = ft + (bxz * bxz - 2.0 * bxz * bzx) * ri * tmag;  // 1360
+                b1 = b1 - W0 * bxz;                        // 1370
+                b2f = b2f - V0 * byy;                      // 1380
+                double d2bxz, d2byz;
+                if (k == 1) {  // 1391, 1511
+                    const double bx2 = fs.xin[R_BX][nc + 2 * g.plane], bx3 = fs.xin[R_BX][nc + 3 * g.plane];
+                    const double by2 = fs.xin[R_BY][nc + 2 * g.plane], by3 = fs.xin[R_BY][nc + 3 * g.plane];
+                    d2bxz = (-3.0 * BX0 + 4.0 * BXzp - bx2) * hz * d2z +
+                            (2.0 * BX0 - 5.0 * BXzp + 4.0 * bx2 - bx3) * h2z * dzk * dzk;
+                    d2byz = (-3.0 * BY0 + 4.0 * BYzp - by2) * hz * d2z +
+                            (2.0 * BY0 - 5.0 * BYzp + 4.0 * by2 - by3) * h2z * dzk * dzk;
+                } else if (k == g.npz) {  // 1392, 1513
+                    const double bx2 = fs.xin[R_BX][nc - 2 * g.plane], bx3 = fs.xin[R_BX][nc - 3 * g.plane];
+                    const double by2 = fs.xin[R_BY][nc - 2 * g.plane], by3 = fs.xin[R_BY][nc - 3 * g.plane];
+                    d2bxz = (3.0 * BX0 - 4.0 * BXzm + bx2) * hz * d2z +
+                            (2.0 * BX0 - 5.0 * BXzm + 4.0 * bx2 - bx3) * h2z * dzk * dzk;
+                    d2byz = (3.0 * BY0 - 4.0 * BYzm + by2) * hz * d2z +
+                            (2.0 * BY0 - 5.0 * BYzm + 4.0 * by2 - by3) * h2z * dzk * dzk;
+                } else {  // 1390, 1510
+                    d2bxz = (BXzp - BXzm) * hz * d2z + (BXzp - 2.0 * BX0 + BXzm) * h2z * dzk * dzk;
+                    d2byz = (BYzp - BYzm) * hz * d2z + (BYzp - 2.0 * BY0 + BYzm) * h2z * dzk * dzk;
+                }
+                const double d2byy = (BYyp - BYym) * hy * d2y + (BYyp - 2.0 * BY0 + BYym) * h2y * dyj * dyj;  // 1400
+                b1 = b1 + orm * d2bxz;                     // 1410
+                b2f = b2f + orm * d2byy;                   // 1420
+                const double byz = (BYzp - BYzm) * hz * dzk;   // 1430
+                const double bzy = (BZyp - BZym) * hy * dyj;   // 1440
+                const double cy = byz - bzy;               // 1450
+                fv = fv + ob * BZ0 * cy;                   // 1460
+                fw = fw - ob * BY0 * cy;                   // 1470
+                ft = ft + (byz * byz + bzy * bzy - 2.0 * byz * bzy) * ri * tmag;  // 1480
+                b2f = b2f - W0 * byz;                      // 1490
+                b3 = b3 - V0 * bzy;                        // 1500
+                const double d2bzy = (BZyp - BZym) * hy * d2y + (BZyp - 2.0 * BZ0 + BZym) * h2y * dyj * dyj;  // 1520
+                b2f = b2f + orm * d2byz;                   // 1530
+                b3 = b3 + orm * d2bzy;                     // 1540
+                const double bzz = (BZzp - BZzm) * hz * dzk;   // 1550
+                b3 = b3 - W0 * bzz;                        // 1560
+                const double d2bzz = (BZzp - BZzm) * hz * d2z + (BZzp - 2.0 * BZ0 + BZzm) * h2z * dzk * dzk;  // 1570
+                b3 = b3 + orm * d2bzz;                     // 1580
+                if (edge) {  // the hydro fluxes there are rewritten by BCON: keep them finite
+                    fu = fv = fw = ft = 0.0;
+                }
+            }
+
+            // ---- stage update, src/step.cpp:53-110 (B: 3dmhdsub.f:957-973, 1059-1075, 1161-1177) ----
+            double F[NF];
+            F[0] = fu;
+            F[1] = fv;
+            F[2] = fw;
+            F[3] = fr;
+            F[4] = ft;
+            if constexpr (MHD) {
+                F[5] = b1;
+                F[6] = b2f;
+                F[7] = b3;
+            }
             const int64_t base = (int64_t)k * g.plane;
-            double xn[5];
+            double xn[NF];
 #pragma unroll
-            for (int f = 0; f < 5; ++f) {
+            for (int f = 0; f < NF; ++f) {
                 const double zv = (STAGE == 0) ? RW_(r0, f, 0, 0) : zq[f];
                 xn[f] = zv + cg * F[f];
                 put_periodic(fs.xout[f], base, g, i, j, xn[f]);
                 if (STAGE < 2) fs.z[f][nc] = xn[f] + cz * F[f];
             }
-            if (STAGE == 2 && k != 1 && k != g.npz) {
+            if (STAGE == 2 && !edge) {
                 const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[k]);
+                double b2sum = 0.0;
+                if constexpr (MHD) b2sum = xn[5] * xn[5] + xn[6] * xn[6] + xn[7] * xn[7];
                 double w1, w2, w3, w4, um;
-                dt_terms<KC>(ph, xn[0], xn[1], xn[2], xn[3], xn[4], 0.0, dd, L.rkapa[k], w1, w2,
+                dt_terms<KC>(ph, xn[0], xn[1], xn[2], xn[3], xn[4], b2sum, dd, L.rkapa[k], w1, w2,
                              w3, w4, um);
                 m1 = fold_min(m1, w1);
                 m2 = fold_min(m2, w2);
                 m3 = fold_min(m3, w3);
+                m4 = fold_min(m4, w4);
                 mu = fold_max(mu, um);
             }
 #undef RW_
@@ -334,30 +467,40 @@ __global__ void __launch_bounds__(NT, kMinBlocks)
     if (STAGE == 2) reduce_dt(der, m1, m2, m3, m4, mu, sc);
 }
 
-template <int STAGE, bool KC>
+template <int STAGE, bool KC, bool MHD>
 static void launch_one(dim3 grid, dim3 block, const StageMaps& maps, const Geometry& g,
                        const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
                        int kchunk, cudaStream_t st) {
     static bool configured = false;
+    constexpr size_t smem = Shape<MHD>::smem;
     if (!configured) {
-        cudaFuncSetAttribute(stage_hydro_fp64<STAGE, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         configured = true;
     }
-    stage_hydro_fp64<STAGE, KC><<<grid, block, kSmem, st>>>(maps, g, ph, L, fs, sc, kchunk);
+    stage_fp64<STAGE, KC, MHD><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
+}
+
+template <bool MHD>
+static void launch_stage(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
+                         const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
+    dim3 block(TX, TY, 1);
+    dim3 grid((g.npx + TX - 1) / TX, (g.npy + TY - 1) / TY, (g.npz + kchunk - 1) / kchunk);
+    const bool kc = ph.kappa_const != 0;
+    if (stage == 0) kc ? launch_one<0, true, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
+                       : launch_one<0, false, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
+    else if (stage == 1) kc ? launch_one<1, true, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
+                            : launch_one<1, false, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
+    else kc ? launch_one<2, true, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
+            : launch_one<2, false, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
 }
 
 cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
                               const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
                               int kchunk, cudaStream_t st) {
-    dim3 block(TX, TY, 1);
-    dim3 grid((g.npx + TX - 1) / TX, (g.npy + TY - 1) / TY, (g.npz + kchunk - 1) / kchunk);
-    const bool kc = ph.kappa_const != 0;
-    if (stage == 0) kc ? launch_one<0, true>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-                       : launch_one<0, false>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
-    else if (stage == 1) kc ? launch_one<1, true>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-                            : launch_one<1, false>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
-    else kc ? launch_one<2, true>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-            : launch_one<2, false>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
+    if (ph.lmag)
+        launch_stage<true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+    else
+        launch_stage<false>(stage, maps, g, ph, L, fs, sc, kchunk, st);
     return cudaGetLastError();
 }
 
