@@ -360,6 +360,8 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
             g->geo.npz = p->npz;
             g->geo.pitch = (d.nx + 15) / 16 * 16;
             g->geo.plane = g->geo.pitch * d.ny;
+            if (g->geo.plane * d.nz >= (int64_t(1) << 31))
+                throw std::invalid_argument("grid too large: a field must hold fewer than 2^31 elements");
             const size_t nbytes = (size_t)g->geo.plane * d.nz * sizeof(double);
             for (int b = 0; b < 2; ++b)
                 for (int q = 0; q < g->nfields; ++q) {

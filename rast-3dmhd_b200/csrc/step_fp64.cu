@@ -143,14 +143,21 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
     const double dx1 = L.dxxdx[ia], d2x = L.d2xxdx2[ia];
     const double dyj = L.dyydy[ja], tmpy = L.tmpy[ja], tmpy1 = L.tmpy1[ja], tmpy2 = L.tmpy2[ja];
 
+    // 32-bit element offsets (a field holds < 2^31 elements, checked at create)
+    const int PL = (int)g.plane, PX = (int)g.pitch;
+    const int col = ja * PX + ia;
+    // offsets from a cell to its periodic ghost images (0: none)
+    const int gdx = (i == 1) ? g.npx : ((i == g.npx) ? -g.npx : 0);
+    const int gdy = (j == 1) ? g.npy * PX : ((j == g.npy) ? -g.npy * PX : 0);
+    const bool ghost = active && (gdx != 0 || gdy != 0);
+
     // RK accumulator Z of the thread's own cell, loaded one plane ahead (registers)
     double zn[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) zn[f] = 0.0;
-    const int64_t col = (int64_t)ja * g.pitch + ia;
     if (STAGE > 0 && active) {
 #pragma unroll
-        for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][(int64_t)kb * g.plane + col];
+        for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][kb * PL + col];
     }
 
     for (int k = kb; k <= ke; ++k) {
@@ -167,10 +174,10 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
         for (int f = 0; f < NF; ++f) zq[f] = zn[f];
         if (STAGE > 0 && active && k < ke) {
 #pragma unroll
-            for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][(int64_t)(k + 1) * g.plane + col];
+            for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][(k + 1) * PL + col];
         }
         if (active) {
-            const int64_t nc = (int64_t)k * g.plane + col;
+            const int nc = k * PL + col;
             const double* rm = raw + ((q + NRAW - 1) % NRAW) * S::raw_slot;
             const double* r0 = raw + (q % NRAW) * S::raw_slot;
             const double* rp = raw + ((q + 1) % NRAW) * S::raw_slot;
@@ -187,9 +194,9 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
             fr -= (RW_(r0, R_RV, 0, 1) - RW_(r0, R_RV, 0, -1)) * tmpy;
             double dwz;
             if (k == 1)
-                dwz = (4.0 * RW_(rp, R_RW, 0, 0) - fs.xin[R_RW][nc + 2 * g.plane]) * tmpz;
+                dwz = (4.0 * RW_(rp, R_RW, 0, 0) - fs.xin[R_RW][nc + 2 * PL]) * tmpz;
             else if (k == g.npz)
-                dwz = (fs.xin[R_RW][nc - 2 * g.plane] - 4.0 * RW_(rm, R_RW, 0, 0)) * tmpz;
+                dwz = (fs.xin[R_RW][nc - 2 * PL] - 4.0 * RW_(rm, R_RW, 0, 0)) * tmpz;
             else
                 dwz = (RW_(rp, R_RW, 0, 0) - RW_(rm, R_RW, 0, 0)) * tmpz;
             fr -= dwz;
@@ -333,11 +340,11 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 // dW/dz with the one-sided forms at the top and bottom planes (2245-2259)
                 double wzb = wz;
                 if (k == 1) {
-                    const int64_t n2 = nc + 2 * g.plane;
+                    const int n2 = nc + 2 * PL;
                     const double w2 = fs.xin[R_RW][n2] * __drcp_rn(fs.xin[R_RO][n2]);
                     wzb = (4.0 * Wzp - w2) * hz * dzk;
                 } else if (k == g.npz) {
-                    const int64_t n2 = nc - 2 * g.plane;
+                    const int n2 = nc - 2 * PL;
                     const double w2 = fs.xin[R_RW][n2] * __drcp_rn(fs.xin[R_RO][n2]);
                     wzb = (w2 - 4.0 * Wzm) * hz * dzk;
                 }
@@ -374,15 +381,15 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 b2f = b2f - V0 * byy;                      // 1380
                 double d2bxz, d2byz;
                 if (k == 1) {  // 1391, 1511
-                    const double bx2 = fs.xin[R_BX][nc + 2 * g.plane], bx3 = fs.xin[R_BX][nc + 3 * g.plane];
-                    const double by2 = fs.xin[R_BY][nc + 2 * g.plane], by3 = fs.xin[R_BY][nc + 3 * g.plane];
+                    const double bx2 = fs.xin[R_BX][nc + 2 * PL], bx3 = fs.xin[R_BX][nc + 3 * PL];
+                    const double by2 = fs.xin[R_BY][nc + 2 * PL], by3 = fs.xin[R_BY][nc + 3 * PL];
                     d2bxz = (-3.0 * BX0 + 4.0 * BXzp - bx2) * hz * d2z +
                             (2.0 * BX0 - 5.0 * BXzp + 4.0 * bx2 - bx3) * h2z * dzk * dzk;
                     d2byz = (-3.0 * BY0 + 4.0 * BYzp - by2) * hz * d2z +
                             (2.0 * BY0 - 5.0 * BYzp + 4.0 * by2 - by3) * h2z * dzk * dzk;
                 } else if (k == g.npz) {  // 1392, 1513
-                    const double bx2 = fs.xin[R_BX][nc - 2 * g.plane], bx3 = fs.xin[R_BX][nc - 3 * g.plane];
-                    const double by2 = fs.xin[R_BY][nc - 2 * g.plane], by3 = fs.xin[R_BY][nc - 3 * g.plane];
+                    const double bx2 = fs.xin[R_BX][nc - 2 * PL], bx3 = fs.xin[R_BX][nc - 3 * PL];
+                    const double by2 = fs.xin[R_BY][nc - 2 * PL], by3 = fs.xin[R_BY][nc - 3 * PL];
                     d2bxz = (3.0 * BX0 - 4.0 * BXzm + bx2) * hz * d2z +
                             (2.0 * BX0 - 5.0 * BXzm + 4.0 * bx2 - bx3) * h2z * dzk * dzk;
                     d2byz = (3.0 * BY0 - 4.0 * BYzm + by2) * hz * d2z +
@@ -426,14 +433,21 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 F[6] = b2f;
                 F[7] = b3;
             }
-            const int64_t base = (int64_t)k * g.plane;
             double xn[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const double zv = (STAGE == 0) ? RW_(r0, f, 0, 0) : zq[f];
                 xn[f] = zv + cg * F[f];
-                put_periodic(fs.xout[f], base, g, i, j, xn[f]);
+                fs.xout[f][nc] = xn[f];
                 if (STAGE < 2) fs.z[f][nc] = xn[f] + cz * F[f];
+            }
+            if (ghost) {  // periodic images (src/communicate.cpp:108-168), edge threads only
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    if (gdx) fs.xout[f][nc + gdx] = xn[f];
+                    if (gdy) fs.xout[f][nc + gdy] = xn[f];
+                    if (gdx && gdy) fs.xout[f][nc + gdx + gdy] = xn[f];
+                }
             }
             if (STAGE == 2 && !edge) {
                 const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[k]);
