@@ -117,7 +117,14 @@ struct r3d_gpu {
     int nfields = 5;
     double* X[2][r3dk::kMaxFields] = {};
     r3dk::StageMaps maps[2];  // TMA maps of X[0] and X[1] (ru rv rw ro tt)
+    r3dk::StageMaps zmaps;    // TMA maps of the FP32 accumulators Z32
     double* Z[r3dk::kMaxFields] = {};
+    // FP32-bulk state (precision == R3D_PREC_FP32BULK): momenta and rho', T' deviations
+    bool fp32 = false;
+    float* X32[2][5] = {};
+    float* Z32[5] = {};
+    r3dk::Background bg{};
+    void* bg_buf = nullptr;
     double* line_buf = nullptr;
     r3dk::Scalars* dsc = nullptr;
     r3dk::Scalars* hsc = nullptr;  // pinned mirror
@@ -154,6 +161,31 @@ FieldSet fieldset(const r3d_gpu* g) {
     return fs;
 }
 
+r3dk::FieldSet32 fieldset32(const r3d_gpu* g) {
+    r3dk::FieldSet32 fs{};
+    for (int q = 0; q < 5; ++q) {
+        fs.xin[q] = g->X32[g->cur][q];
+        fs.xout[q] = g->X32[1 - g->cur][q];
+        fs.z[q] = g->Z32[q];
+    }
+    return fs;
+}
+
+// R(k), T0(k) over the global z index: ghost 0 -> T(0), interior k -> T(k-1), ghost npz+1 -> the
+// bottom value (src/static_ic.cpp:53-89 stitched over ranks).
+void background_columns(const r3d_params& p, std::vector<double>& R, std::vector<double>& T) {
+    std::vector<double> t, r;
+    static_profile(p, t, r);
+    const int nz = p.npz + 2;
+    R.assign(nz, 0.0);
+    T.assign(nz, 0.0);
+    for (int k = 0; k < nz; ++k) {
+        const int src = k == 0 ? 0 : (k == nz - 1 ? p.npz - 1 : k - 1);
+        R[k] = r[src];
+        T[k] = t[src];
+    }
+}
+
 double plume_tpr(const r3d_gpu* g) {
     const double timt = g->host_timc + g->host_timi;  // src/bcon.cpp:22
     return (g->p.tc != 0.0) ? g->p.tp + (1.0 - g->p.tp) * std::exp(-timt / g->p.tc) : g->p.tp;
@@ -184,6 +216,13 @@ struct Timer {
     }
 };
 
+void launch_dt_full_any(r3d_gpu* g) {
+    if (g->fp32)
+        cuda_ok(r3dk::launch_dt_full_fp32(g->geo, g->ph, g->lines, g->bg, fieldset32(g), g->dsc, g->stream), "dt_full32");
+    else
+        cuda_ok(r3dk::launch_dt_full(g->geo, g->ph, g->lines, fieldset(g), g->dsc, g->stream), "dt_full");
+}
+
 // Queue one step (nstages substages) on the device.
 void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_launches) {
     g->bnd.tpr = plume_tpr(g);
@@ -192,12 +231,20 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
     tm.end(2);
     ++launches;
     for (int s = 0; s < nstages; ++s) {
-        FieldSet fs = fieldset(g);
         tm.begin();
-        cuda_ok(r3dk::launch_stage_fp64(s, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage");
-        tm.end(0);
-        tm.begin();
-        cuda_ok(r3dk::launch_bcon(g->geo, g->ph, g->lines, g->bnd, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon");
+        if (g->fp32) {
+            r3dk::FieldSet32 fs = fieldset32(g);
+            cuda_ok(r3dk::launch_stage_fp32(s, g->maps[g->cur], g->zmaps, g->geo, g->ph, g->lines, g->bg, fs, g->dsc, g->kchunk, g->stream), "stage32");
+            tm.end(0);
+            tm.begin();
+            cuda_ok(r3dk::launch_bcon_fp32(g->geo, g->ph, g->lines, g->bnd, g->bg, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon32");
+        } else {
+            FieldSet fs = fieldset(g);
+            cuda_ok(r3dk::launch_stage_fp64(s, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage");
+            tm.end(0);
+            tm.begin();
+            cuda_ok(r3dk::launch_bcon(g->geo, g->ph, g->lines, g->bnd, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon");
+        }
         tm.end(1);
         launches += 2;
         ++stage_launches;
@@ -207,8 +254,7 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
     cuda_ok(r3dk::launch_step_end(g->dsc, g->stream), "step_end");
     ++launches;
     if (nstages < 3) {  // the next dt needs the limits of this (partial-step) state
-        FieldSet fs = fieldset(g);
-        cuda_ok(r3dk::launch_dt_full(g->geo, g->ph, g->lines, fs, g->dsc, g->stream), "dt_full");
+        launch_dt_full_any(g);
         ++launches;
     }
     tm.end(2);
@@ -334,6 +380,66 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
     g->bnd.dz_bot = dzs / st->dzzdz[p.npz];        // src/bcon.cpp:124
 }
 
+// FP32-bulk background tables (see r3dk::Background).
+void upload_background(r3d_gpu* g, const r3d_host_state* st) {
+    const r3d_params& p = g->p;
+    const Derived& d = g->d;
+    const int64_t NZ = d.nz;
+    std::vector<double> R, T;
+    background_columns(p, R, T);
+    std::vector<double> hres(NZ, 0.0), dt0(NZ, 0.0), lt0(NZ, 0.0);
+    for (int64_t k = 1; k < NZ - 1; ++k) {
+        const double tz = d.hz * st->dzzdz[k];
+        const double tz1 = d.hz * st->d2zzdz2[k];
+        const double tz2 = d.h2z * st->dzzdz[k] * st->dzzdz[k];
+        hres[k] = p.grav * R[k] - (R[k + 1] * T[k + 1] - R[k - 1] * T[k - 1]) * tz;
+        dt0[k] = T[k + 1] - T[k - 1];
+        lt0[k] = dt0[k] * tz1 + (T[k + 1] - 2.0 * T[k] + T[k - 1]) * tz2;
+    }
+    const size_t nd = (size_t)NZ, pad = (nd + 15) / 16 * 16;
+    const size_t bytes = pad * (5 * sizeof(double) + 2 * sizeof(float)) + nd * 12 * sizeof(float);
+    if (!g->bg_buf) {
+        cuda_ok(cudaMalloc(&g->bg_buf, bytes), "cudaMalloc(background)");
+        g->bytes += bytes;
+    }
+    std::vector<unsigned char> host(bytes, 0);
+    double* hd = reinterpret_cast<double*>(host.data());
+    const std::vector<double>* cols[5] = {&R, &T, &hres, &dt0, &lt0};
+    for (int c = 0; c < 5; ++c) std::memcpy(hd + c * pad, cols[c]->data(), nd * sizeof(double));
+    float* hf = reinterpret_cast<float*>(hd + 5 * pad);
+    for (size_t k = 0; k < nd; ++k) {
+        hf[k] = (float)R[k];
+        hf[pad + k] = (float)T[k];
+    }
+    float* kf = hf + 2 * pad;  // 12 floats per plane (3 x float4), 16-byte aligned
+    for (size_t k = 0; k < nd; ++k) {
+        float* e = kf + 12 * k;
+        e[0] = (float)(d.hz * st->dzzdz[k]);
+        e[1] = (float)(d.hz * st->d2zzdz2[k]);
+        e[2] = (float)(d.h2z * st->dzzdz[k] * st->dzzdz[k]);
+        e[3] = (float)(d.hz * st->dzzdz[k]);
+        e[4] = (float)hres[k];
+        e[5] = (float)dt0[k];
+        e[6] = (float)lt0[k];
+        e[7] = (float)st->rkapa[k];
+        e[8] = (float)st->dkapa[k];
+        e[9] = (float)R[k];
+        e[10] = (float)T[k];
+        e[11] = 0.0f;
+    }
+    cuda_ok(cudaMemcpy(g->bg_buf, host.data(), host.size(), cudaMemcpyHostToDevice), "upload background");
+    const double* dd = static_cast<const double*>(g->bg_buf);
+    const float* df = reinterpret_cast<const float*>(dd + 5 * pad);
+    g->bg.r = dd;
+    g->bg.t = dd + pad;
+    g->bg.hres = dd + 2 * pad;
+    g->bg.dt0 = dd + 3 * pad;
+    g->bg.lt0 = dd + 4 * pad;
+    g->bg.rf = df;
+    g->bg.tf = df + pad;
+    g->bg.kf = reinterpret_cast<const float4*>(df + 2 * pad);
+}
+
 }  // namespace
 
 extern "C" {
@@ -362,22 +468,49 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
             g->geo.plane = g->geo.pitch * d.ny;
             if (g->geo.plane * d.nz >= (int64_t(1) << 31))
                 throw std::invalid_argument("grid too large: a field must hold fewer than 2^31 elements");
-            const size_t nbytes = (size_t)g->geo.plane * d.nz * sizeof(double);
-            for (int b = 0; b < 2; ++b)
+            g->fp32 = p->precision == R3D_PREC_FP32BULK;
+            if (g->fp32) {
+                g->geo.pitch = (d.nx + 31) / 32 * 32;  // 128-byte rows of floats
+                g->geo.plane = g->geo.pitch * d.ny;
+                const size_t nb = (size_t)g->geo.plane * d.nz * sizeof(float);
+                for (int b = 0; b < 2; ++b)
+                    for (int q = 0; q < 5; ++q) {
+                        cuda_ok(cudaMalloc(&g->X32[b][q], nb), "cudaMalloc(state32)");
+                        g->bytes += nb;
+                    }
+                for (int q = 0; q < 5; ++q) {
+                    cuda_ok(cudaMalloc(&g->Z32[q], nb), "cudaMalloc(accumulator32)");
+                    cuda_ok(cudaMemsetAsync(g->Z32[q], 0, nb, g->stream), "cudaMemset");
+                    g->bytes += nb;
+                }
+                unsigned bx = 0, by = 0;
+                r3dk::stage_fp32_box(&bx, &by);
+                for (int b = 0; b < 2; ++b)
+                    for (int q = 0; q < 5; ++q)
+                        g->maps[b].m[q] = field_map(g->X32[b][q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
+                                                    bx, by, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float));
+                r3dk::stage_fp32_zbox(&bx, &by);
+                for (int q = 0; q < 5; ++q)  // Z rows start at interior column 1
+                    g->zmaps.m[q] = field_map(g->Z32[q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
+                                              bx, by, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float));
+            } else {
+                const size_t nbytes = (size_t)g->geo.plane * d.nz * sizeof(double);
+                for (int b = 0; b < 2; ++b)
+                    for (int q = 0; q < g->nfields; ++q) {
+                        cuda_ok(cudaMalloc(&g->X[b][q], nbytes), "cudaMalloc(state)");
+                        g->bytes += nbytes;
+                    }
+                unsigned bx = 0, by = 0;
+                r3dk::stage_fp64_box(&bx, &by);  // the box the stage kernel expects per plane
+                for (int b = 0; b < 2; ++b)
+                    for (int q = 0; q < g->nfields; ++q)
+                        g->maps[b].m[q] = field_map(g->X[b][q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
+                                                    bx, by, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double));
                 for (int q = 0; q < g->nfields; ++q) {
-                    cuda_ok(cudaMalloc(&g->X[b][q], nbytes), "cudaMalloc(state)");
+                    cuda_ok(cudaMalloc(&g->Z[q], nbytes), "cudaMalloc(accumulator)");
+                    cuda_ok(cudaMemsetAsync(g->Z[q], 0, nbytes, g->stream), "cudaMemset");
                     g->bytes += nbytes;
                 }
-            unsigned bx = 0, by = 0;
-            r3dk::stage_fp64_box(&bx, &by);  // the box the stage kernel expects per plane
-            for (int b = 0; b < 2; ++b)
-                for (int q = 0; q < g->nfields; ++q)
-                    g->maps[b].m[q] = field_map(g->X[b][q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
-                                                bx, by, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double));
-            for (int q = 0; q < g->nfields; ++q) {
-                cuda_ok(cudaMalloc(&g->Z[q], nbytes), "cudaMalloc(accumulator)");
-                cuda_ok(cudaMemsetAsync(g->Z[q], 0, nbytes, g->stream), "cudaMemset");
-                g->bytes += nbytes;
             }
             cuda_ok(cudaMalloc(&g->dsc, sizeof(r3dk::Scalars)), "cudaMalloc(scalars)");
             cuda_ok(cudaMallocHost(&g->hsc, sizeof(r3dk::Scalars)), "cudaMallocHost");
@@ -424,6 +557,10 @@ int r3d_gpu_destroy(r3d_gpu* g) {
     for (int b = 0; b < 2; ++b)
         for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->X[b][q]);
     for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->Z[q]);
+    for (int b = 0; b < 2; ++b)
+        for (int q = 0; q < 5; ++q) cudaFree(g->X32[b][q]);
+    for (int q = 0; q < 5; ++q) cudaFree(g->Z32[q]);
+    cudaFree(g->bg_buf);
     cudaFree(g->line_buf);
     cudaFree(g->dsc);
     if (g->hsc) cudaFreeHost(g->hsc);
@@ -446,12 +583,32 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
         for (auto l : lines)
             if (!l) throw std::invalid_argument("r3d_host_state metric line is NULL");
         upload_lines(g, st);
-        for (int b = 0; b < 2; ++b)
-            for (int q = 0; q < g->nfields; ++q)
-                cuda_ok(cudaMemcpy2DAsync(g->X[b][q], g->geo.pitch * sizeof(double), src[q],
-                                          d.nx * sizeof(double), d.nx * sizeof(double), d.ny * d.nz,
-                                          cudaMemcpyHostToDevice, g->stream),
-                        "upload state");
+        if (g->fp32) {
+            upload_background(g, st);
+            std::vector<double> R, T;
+            background_columns(g->p, R, T);
+            const int64_t NX = d.nx, NY = d.ny, NZ = d.nz, per = NX * NY;
+            std::vector<float> tmp((size_t)(per * NZ));
+            for (int q = 0; q < 5; ++q) {
+                for (int64_t k = 0; k < NZ; ++k) {
+                    const double bgv = q == 3 ? R[k] : (q == 4 ? T[k] : 0.0);
+                    const double* a = src[q] + k * per;
+                    float* o = tmp.data() + k * per;
+                    for (int64_t n = 0; n < per; ++n) o[n] = (float)(a[n] - bgv);
+                }
+                for (int b = 0; b < 2; ++b)
+                    cuda_ok(cudaMemcpy2D(g->X32[b][q], g->geo.pitch * sizeof(float), tmp.data(),
+                                         NX * sizeof(float), NX * sizeof(float), NY * NZ, cudaMemcpyHostToDevice),
+                            "upload state32");
+            }
+        } else {
+            for (int b = 0; b < 2; ++b)
+                for (int q = 0; q < g->nfields; ++q)
+                    cuda_ok(cudaMemcpy2DAsync(g->X[b][q], g->geo.pitch * sizeof(double), src[q],
+                                              d.nx * sizeof(double), d.nx * sizeof(double), d.ny * d.nz,
+                                              cudaMemcpyHostToDevice, g->stream),
+                            "upload state");
+        }
         g->cur = 0;
         r3dk::Scalars h{};
         h.dt = sc->dt; h.timc = sc->timc; h.timt = sc->timt; h.timi = sc->timi;
@@ -462,8 +619,7 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
         g->host_timc = sc->timc;
         g->host_timi = sc->timi;
         cuda_ok(r3dk::launch_reset_reduction(g->dsc, g->stream), "reset");
-        FieldSet fs = fieldset(g);
-        cuda_ok(r3dk::launch_dt_full(g->geo, g->ph, g->lines, fs, g->dsc, g->stream), "dt_full");
+        launch_dt_full_any(g);
         cuda_ok(cudaStreamSynchronize(g->stream), "upload");
         g->uploaded = true;
     });
@@ -476,12 +632,30 @@ int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc) {
         DeviceGuard dg(g->device);
         const Derived& d = g->d;
         double* dst[r3dk::kMaxFields] = {st->ru, st->rv, st->rw, st->ro, st->tt, st->bx, st->by, st->bz};
-        for (int q = 0; q < g->nfields; ++q) {
-            if (!dst[q]) continue;
-            cuda_ok(cudaMemcpy2DAsync(dst[q], d.nx * sizeof(double), g->X[g->cur][q],
-                                      g->geo.pitch * sizeof(double), d.nx * sizeof(double), d.ny * d.nz,
-                                      cudaMemcpyDeviceToHost, g->stream),
-                    "download state");
+        if (g->fp32) {
+            std::vector<double> R, T;
+            background_columns(g->p, R, T);
+            const int64_t NX = d.nx, NY = d.ny, NZ = d.nz, per = NX * NY;
+            std::vector<float> tmp((size_t)(per * NZ));
+            cuda_ok(cudaStreamSynchronize(g->stream), "download");
+            for (int q = 0; q < 5; ++q) {
+                if (!dst[q]) continue;
+                cuda_ok(cudaMemcpy2D(tmp.data(), NX * sizeof(float), g->X32[g->cur][q], g->geo.pitch * sizeof(float),
+                                     NX * sizeof(float), NY * NZ, cudaMemcpyDeviceToHost),
+                        "download state32");
+                for (int64_t k = 0; k < NZ; ++k) {
+                    const double bgv = q == 3 ? R[k] : (q == 4 ? T[k] : 0.0);
+                    for (int64_t n = 0; n < per; ++n) dst[q][k * per + n] = bgv + (double)tmp[k * per + n];
+                }
+            }
+        } else {
+            for (int q = 0; q < g->nfields; ++q) {
+                if (!dst[q]) continue;
+                cuda_ok(cudaMemcpy2DAsync(dst[q], d.nx * sizeof(double), g->X[g->cur][q],
+                                          g->geo.pitch * sizeof(double), d.nx * sizeof(double), d.ny * d.nz,
+                                          cudaMemcpyDeviceToHost, g->stream),
+                        "download state");
+            }
         }
         pull_scalars(g, sc);
     });
@@ -532,8 +706,10 @@ int r3d_gpu_totals(r3d_gpu* g, double* mass, double* energy) {
         DeviceGuard dg(g->device);
         double zero[2] = {0.0, 0.0};
         cuda_ok(cudaMemcpyAsync(&g->dsc->mass, zero, sizeof(zero), cudaMemcpyHostToDevice, g->stream), "totals");
-        FieldSet fs = fieldset(g);
-        cuda_ok(r3dk::launch_totals(g->geo, g->ph, fs, g->dsc, g->stream), "totals");
+        if (g->fp32)
+            cuda_ok(r3dk::launch_totals_fp32(g->geo, g->ph, g->bg, fieldset32(g), g->dsc, g->stream), "totals32");
+        else
+            cuda_ok(r3dk::launch_totals(g->geo, g->ph, fieldset(g), g->dsc, g->stream), "totals");
         cuda_ok(cudaMemcpyAsync(zero, &g->dsc->mass, sizeof(zero), cudaMemcpyDeviceToHost, g->stream), "totals");
         cuda_ok(cudaStreamSynchronize(g->stream), "totals");
         if (mass) *mass = zero[0];

@@ -30,6 +30,33 @@ struct StageMaps {
     CUtensorMap m[kMaxFields];
 };
 
+// Static background of the FP32-bulk form: R(k), T0(k) of the polytrope over the global z
+// index (FP64 and FP32 copies) and the per-plane background parts of the z terms, in FP64:
+// hres = g*R - (R*T0)_z (hydrostatic residual), dt0 = T0(k+1) - T0(k-1),
+// lt0 = dt0*tmpz1 + (T0(k+1) - 2*T0(k) + T0(k-1))*tmpz2.
+struct Background {
+    const double *r, *t, *hres, *dt0, *lt0;
+    const float *rf, *tf;
+    const float4* kf;  // per plane, 3 x float4: {tmpz, tmpz1, tmpz2, hz*dzzdz}, {hres, dt0, lt0, rkapa},
+                       // {dkapa, R, T0, 0}
+};
+
+void stage_fp32_box(unsigned* bx, unsigned* by);
+// Z box of the FP32 stage kernel: Z is stored one column left-shifted (element (i,j,k) at
+// k*plane + j*pitch + i-1) so an interior tile starts on a 16-byte boundary.
+void stage_fp32_zbox(unsigned* bx, unsigned* by);
+cudaError_t launch_stage_fp32(int stage, const StageMaps& maps, const StageMaps& zmaps,
+                              const Geometry& g, const Physics& ph, const Lines& L,
+                              const Background& bg, const FieldSet32& fs, Scalars* sc, int kchunk,
+                              cudaStream_t st);
+cudaError_t launch_bcon_fp32(const Geometry& g, const Physics& ph, const Lines& L, const Boundary& b,
+                             const Background& bg, const FieldSet32& fs, Scalars* sc, int with_dt,
+                             cudaStream_t st);
+cudaError_t launch_dt_full_fp32(const Geometry& g, const Physics& ph, const Lines& L,
+                                const Background& bg, const FieldSet32& fs, Scalars* sc, cudaStream_t st);
+cudaError_t launch_totals_fp32(const Geometry& g, const Physics& ph, const Background& bg,
+                               const FieldSet32& fs, Scalars* sc, cudaStream_t st);
+
 size_t stage_fp64_smem();
 // TMA box (x, y) of one field plane that the FP64 stage kernel was compiled for.
 void stage_fp64_box(unsigned* bx, unsigned* by);

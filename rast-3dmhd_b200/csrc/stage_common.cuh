@@ -32,6 +32,42 @@ __device__ __forceinline__ void dt_terms(const Physics& ph, double ru, double rv
     w3 = 0.375 * dd * dd * ph.re * ro;
 }
 
+// std::min(acc, v) / std::max(acc, v): a NaN v never replaces acc.
+__device__ __forceinline__ double fold_min(double acc, double v);
+__device__ __forceinline__ double fold_max(double acc, double v);
+
+// Fold one cell's time-step limits into running minima m1..m4 and maximum mu, evaluating the
+// costly FP64 ww1 = dd/sqrt(c^2) and Mach term (a reciprocal, two divisions, two square roots)
+// only for cells that can change m1 or mu.  FP32 estimates of both, with relative error below
+// 2^-18 (about twenty float operations on positive quantities, each correctly rounded or within
+// 2 ulp), are compared with the running values under a 2^-12 margin: a cell whose estimate is
+// clearly worse cannot be the minimum (maximum) and is skipped; every other cell - including any
+// cell whose estimate is not finite, and every cell while the running maximum is below 1e-30,
+// where float underflow voids the bound - takes the FP64 path.  The running values therefore
+// equal those of folding the FP64 values of every cell.
+__device__ __forceinline__ void fold_dt_terms_filtered(const Physics& ph, double ru, double rv,
+                                                       double rw, double ro, double tt, double dd,
+                                                       double rkap, double& m1, double& m2,
+                                                       double& m3, double& mu) {
+    m2 = fold_min(m2, 0.5 * dd * dd * ph.repr * ph.cv * ro / rkap);  // src/step.cpp:192-193
+    m3 = fold_min(m3, 0.375 * dd * dd * ph.re * ro);                 // src/step.cpp:194
+    const float rof = (float)ro, ttf = (float)tt;
+    const float ruf = (float)ru, rvf = (float)rv, rwf = (float)rw;
+    const float rf = __fdividef(1.0f, rof);
+    const float uuf = (ruf * ruf + rvf * rvf + rwf * rwf) * rf * rf;
+    const float umf = __fdividef((float)ph.ogamma * uuf, ttf);
+    const float gtf = (float)ph.gamma * ttf;
+    const float c2f = uuf + gtf + 2.0f * sqrtf(uuf * gtf);
+    const float w1f = __fdividef((float)dd, sqrtf(c2f));
+    const bool skip_um = (double)umf * (1.0 + 1.0 / 4096.0) < mu && mu > 1e-30;
+    const bool skip_w1 = (double)w1f * (1.0 - 1.0 / 4096.0) > m1;
+    if (skip_um && skip_w1) return;
+    double w1, w2, w3, w4, um;
+    dt_terms<false>(ph, ru, rv, rw, ro, tt, 0.0, dd, rkap, w1, w2, w3, w4, um);
+    m1 = fold_min(m1, w1);
+    mu = fold_max(mu, um);
+}
+
 // std::min(std::min(a, b), c) with the reference's comparison order.
 __device__ __forceinline__ double min_of3(double a, double b, double c) {
     const double m = (b < a) ? b : a;

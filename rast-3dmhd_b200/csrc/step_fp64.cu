@@ -59,6 +59,7 @@ struct Shape {
     static constexpr uint32_t plane_tx = nf * SN * sizeof(double);  // TMA bytes per plane
     static constexpr size_t smem = raw_bytes + der_bytes + 64;
     static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && NT <= 256) ? 2 : 1;
+    static_assert(raw_bytes % 128 == 0 && (RAWF * 8) % 128 == 0, "TMA destinations 128-byte aligned");
 };
 }  // namespace
 
