@@ -196,6 +196,29 @@ def cpu_reference_sample(max_seconds: float = 20.0):
                           f"{nsteps} steps ({e})"}
 
 
+def side_run(R, flags, steps, warmup, bytes_per_cell, fp64_ms_per_step):
+    """Timed run of another form of the step (same protocol as the headline, events on the
+    library stream); returns Mcell-updates/s, % of the HBM roofline by its own algorithmic bytes
+    and, for FP32-bulk, the speed-up over the FP64 headline run."""
+    p = R.parse(flags)
+    npx, npy, npz = p.npx, p.npy, p.npz
+    st = R.HostState.setup(p)
+    with R.GpuSim(p) as sim:
+        sim.upload(st)
+        sim.run(warmup)
+        _, tm = sim.run_timed(steps)
+    cells = npx * npy * npz
+    ms = tm["total_ms"] / steps
+    peak, _ = peak_hbm()
+    out = {"value": cells / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms, "steps": steps,
+           "grid": [npx, npy, npz], "bytes_per_cell_step": bytes_per_cell,
+           "hbm_frac": bytes_per_cell * cells / (ms / 1e3) / 1e9 / peak,
+           "stage_kernel_ms": tm["stage_ms"] / max(1, tm["stage_launches"])}
+    if fp64_ms_per_step:
+        out["speedup_vs_fp64"] = fp64_ms_per_step / ms
+    return out
+
+
 def run_reference_arm(args, world, rank, pg):
     if rank != 0:
         return 0
@@ -240,6 +263,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the FP32-bulk and MHD side measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -304,10 +328,19 @@ def main():
                 "kernel": "stage_hydro_fp64 (fused FLUXES + RK3 stage update)",
                 "step_frac": (cells * BYTES_PER_CELL_STEP / (ms_per_step / 1e3) / 1e9) / peak}
 
+    sim.close()
+    extra = {}
+    if not args.no_extra:
+        extra["fp32bulk_504x504x512"] = side_run(R, FLAGS + ["--seed", str(SEED), "--precision", "fp32bulk",
+                                                             "--gpu", str(local)], args.steps, args.warmup,
+                                                 200.0, ms_per_step)
+        extra["mhd_fp64_126x126x256"] = side_run(R, ["--npx", "126", "--npy", "126", "--npz", "256", "--lmag", "1",
+                                                     "--beta", "10", "--rm", "1", "--ampb", "0.1", "--bfh", "2",
+                                                     "--bzp", "20", "--seed", "7", "--gpu", str(local)],
+                                                 max(args.steps, 20), args.warmup, 640.0, None)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu = cpu_reference_sample()
-    sim.close()
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -319,7 +352,7 @@ def main():
                           "parallelism": f"{world} replica(s), one GPU each"},
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": int(tm["total_launches"]), "clocks": clk.summary(),
-               "final_dt": sc["dt"]}
+               "final_dt": sc["dt"], "extra": extra}
         print(json.dumps(out))
     if pg is not None:
         pg.destroy_process_group()
