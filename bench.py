@@ -94,6 +94,14 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first(self, limit_s: float = 5.0):
+        """Block until nvidia-smi has produced a sample (it takes a moment to start), then drop
+        the samples taken so far so that the summary covers the timed region only."""
+        t0 = time.perf_counter()
+        while self.proc and not self.lines and time.perf_counter() - t0 < limit_s:
+            time.sleep(0.02)
+        self.lines = []
+
     def __exit__(self, *a):
         if self.proc:
             self.proc.terminate()
@@ -259,12 +267,20 @@ def run_reference_arm(args, world, rank, pg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the FP32-bulk and MHD side measurements")
+    ap.add_argument("--grid", type=int, nargs=3, metavar=("NPX", "NPY", "NPZ"),
+                    help="another grid (small cases for profiling); the default is the benchmark grid")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32bulk"],
+                    help="form of the headline run (fp64 is the benchmark; fp32bulk for profiling)")
     args = ap.parse_args()
+    global GRID, FLAGS
+    if args.grid:
+        GRID = tuple(args.grid)
+        FLAGS = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(GRID[2])]
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_init()
@@ -278,14 +294,17 @@ def main():
 
     import r3d_b200 as R
 
-    p = R.parse(FLAGS + ["--seed", str(SEED), "--gpu", str(local)])
+    p = R.parse(FLAGS + ["--seed", str(SEED), "--gpu", str(local), "--precision", args.precision])
     cells = GRID[0] * GRID[1] * GRID[2]
+    fp32 = args.precision == "fp32bulk"
+    bytes_step = 200.0 if fp32 else BYTES_PER_CELL_STEP
     st = R.HostState.setup(p)
     sim = R.GpuSim(p)
     sim.upload(st)
-    sim.run(args.warmup)                         # untimed warm-up
-    barrier(pg)
     with ClockSampler(local) as clk:
+        sim.run(args.warmup)                     # untimed warm-up
+        clk.wait_first()
+        barrier(pg)
         sc, tm = sim.run_timed(args.steps)       # synchronises on exit
     barrier(pg)
     total_ms = allmax(pg, tm["total_ms"])
@@ -320,17 +339,17 @@ def main():
                    "per-step scalar read-back"}
 
     peak, peak_kind = peak_hbm()
-    alg_bytes_launch = cells * BYTES_PER_CELL_STAGE
+    alg_bytes_launch = cells * bytes_step / 3.0
     achieved = alg_bytes_launch / (stage_avg_ms / 1e3) / 1e9
-    traffic = stage_traffic_per_launch(cells)
+    traffic = None if fp32 else stage_traffic_per_launch(cells)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
-                "kernel": "stage_hydro_fp64 (fused FLUXES + RK3 stage update)",
-                "step_frac": (cells * BYTES_PER_CELL_STEP / (ms_per_step / 1e3) / 1e9) / peak}
+                "kernel": ("stage_fp32" if fp32 else "stage_fp64") + " (fused FLUXES + RK3 stage update)",
+                "step_frac": (cells * bytes_step / (ms_per_step / 1e3) / 1e9) / peak}
 
     sim.close()
     extra = {}
-    if not args.no_extra:
+    if not args.no_extra and not args.grid and not fp32:
         extra["fp32bulk_504x504x512"] = side_run(R, FLAGS + ["--seed", str(SEED), "--precision", "fp32bulk",
                                                              "--gpu", str(local)], args.steps, args.warmup,
                                                  200.0, ms_per_step)
@@ -344,10 +363,11 @@ def main():
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": f"FP64 hydro {GRID[0]}x{GRID[1]}x{GRID[2]}, default physics, "
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if fp32 else "f64",
+               "data": "synthetic",
+               "config": {"workload": f"{'FP32-bulk' if fp32 else 'FP64'} hydro {GRID[0]}x{GRID[1]}x{GRID[2]}, default physics, "
                                       f"polytrope + RAN2 seed {SEED} ampt 0.005",
-                          "grid": list(GRID), "precision": "fp64", "bit_exact": True,
+                          "grid": list(GRID), "precision": args.precision, "bit_exact": not fp32,
                           "l2": "inputs 16 GB >> 126 MB L2 (no flush needed)",
                           "parallelism": f"{world} replica(s), one GPU each"},
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
