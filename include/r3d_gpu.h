@@ -128,6 +128,30 @@ int r3d_gpu_run_timed(r3d_gpu* g, int nsteps, r3d_scalars* sc, r3d_timing* tm);
  * the device (mass = sum rho, energy = sum (rho*T*cv + 0.5*(ru^2+rv^2+rw^2)/rho)). */
 int r3d_gpu_totals(r3d_gpu* g, double* mass, double* energy);
 
+/* ---- discrete adjoint of the RK3 step (FP64; no counterpart in the reference) ----
+ * Reverse-mode derivative of exactly the map r3d_gpu_run computes (FLUXES, the stage update,
+ * BCON, the periodic ghost images and the dt minimum of src/step.cpp:114-257), with state
+ * checkpoints on the device.  Cotangent arrays use the host layout of r3d_host_state fields:
+ * one pointer per field in the order ru rv rw ro tt (+ bx by bz with lmag), each NX*NY*NZ
+ * doubles.  Requires precision FP64 and a time-independent top boundary (tc == 0), else
+ * R3D_EINVAL.  The derivative is taken w.r.t. the interior values of the starting state, whose
+ * x/y ghost cells are the periodic images of the interior (as upload and every step leave
+ * them); gradients are returned on interior cells, ghost entries 0.  dt = sff*min(limits)
+ * contributes the derivative of the limit at the cell that sets it (lowest cell index on a
+ * tie); at a cell at rest the momentum derivative of the CFL limit is taken as 0. */
+/* Run nsteps (>= 1) forward from the current device state, as r3d_gpu_run does, keeping the
+ * state every checkpoint_every steps (and the final state) for r3d_gpu_adjoint_backward.  The
+ * simulation is left at the final state; later steps do not disturb the recording. */
+int r3d_gpu_adjoint_record(r3d_gpu* g, int nsteps, int checkpoint_every, r3d_scalars* sc);
+/* Given the cotangent of the recorded final state (seed), the cotangent of the recorded
+ * starting state (grad).  Each segment is recomputed from its checkpoint; a recomputed state
+ * that differs from the recorded one by a single bit gives R3D_ENUMERIC. */
+int r3d_gpu_adjoint_backward(r3d_gpu* g, const double* const* seed, double* const* grad);
+/* One-step vector-Jacobian product at the current device state (the state is not advanced). */
+int r3d_gpu_adjoint_step(r3d_gpu* g, const double* const* seed, double* const* grad);
+/* Device bytes held by the adjoint workspace and checkpoints (0 before first use). */
+int r3d_gpu_adjoint_memory(const r3d_gpu* g, int64_t* bytes);
+
 /* ---- allocation-free time-step limits (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc (for example a program that reserves the GPU's memory
  * in its own pool up front, or a time loop that must not pay the device synchronisation that

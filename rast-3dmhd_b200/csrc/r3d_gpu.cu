@@ -24,17 +24,13 @@
 #include "r3d_gpu.h"
 #include "r3d_host.hpp"
 #include "r3d_kernels.h"
+#include "r3d_gpu_impl.hpp"
 
 using namespace r3db;
+using namespace r3dg;
 using r3dk::FieldSet;
 
 namespace {
-
-inline void cuda_ok(cudaError_t e, const char* what) {
-    if (e != cudaSuccess)
-        throw Error(e == cudaErrorMemoryAllocation ? R3D_ENOMEM : R3D_ECUDA,
-                    std::string(what) + ": " + cudaGetErrorString(e));
-}
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed).
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
@@ -54,6 +50,10 @@ EncodeTiled encode_fn() {
     return fn;
 }
 
+}  // namespace
+
+namespace r3dg {
+
 // 3D map over one padded field: dims (npx+2, npy+2, npz+2), box (34, 10, 1).  Reads past the
 // x/y extent of the last tiles are zero-filled by the TMA unit and never used.
 CUtensorMap field_map(void* base, int64_t nx, int64_t ny, int64_t nz, int64_t pitch, int64_t plane,
@@ -69,6 +69,10 @@ CUtensorMap field_map(void* base, int64_t nx, int64_t ny, int64_t nz, int64_t pi
     if (r != CUDA_SUCCESS) throw Error(R3D_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
     return m;
 }
+
+}  // namespace r3dg
+
+namespace {
 
 __global__ void totals_kernel(r3dk::Geometry g, r3dk::Physics ph, FieldSet fs, r3dk::Scalars* sc) {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -105,51 +109,7 @@ cudaError_t launch_totals(const Geometry& g, const Physics& ph, const FieldSet& 
 }
 }  // namespace r3dk
 
-struct r3d_gpu {
-    r3d_params p;
-    Derived d;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    r3dk::Geometry geo{};
-    r3dk::Physics ph{};
-    r3dk::Lines lines{};
-    r3dk::Boundary bnd{};
-    int nfields = 5;
-    double* X[2][r3dk::kMaxFields] = {};
-    r3dk::StageMaps maps[2];  // TMA maps of X[0] and X[1] (ru rv rw ro tt)
-    r3dk::StageMaps zmaps;    // TMA maps of the FP32 accumulators Z32
-    double* Z[r3dk::kMaxFields] = {};
-    // FP32-bulk state (precision == R3D_PREC_FP32BULK): momenta and rho', T' deviations
-    bool fp32 = false;
-    float* X32[2][5] = {};
-    float* Z32[5] = {};
-    r3dk::Background bg{};
-    void* bg_buf = nullptr;
-    double* line_buf = nullptr;
-    r3dk::Scalars* dsc = nullptr;
-    r3dk::Scalars* hsc = nullptr;  // pinned mirror
-    int cur = 0;
-    int kchunk = 32;
-    bool uploaded = false;
-    int64_t bytes = 0;
-    double host_timc = 0.0, host_timi = 0.0;  // host clock for the plume relaxation (tc != 0)
-    std::vector<cudaEvent_t> ev;             // timing events (r3d_gpu_run_timed)
-};
-
-namespace {
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int now = -1;
-        cudaGetDevice(&now);
-        if (prev >= 0 && now != prev) cudaSetDevice(prev);
-    }
-};
+namespace r3dg {
 
 FieldSet fieldset(const r3d_gpu* g) {
     FieldSet fs{};
@@ -190,31 +150,6 @@ double plume_tpr(const r3d_gpu* g) {
     const double timt = g->host_timc + g->host_timi;  // src/bcon.cpp:22
     return (g->p.tc != 0.0) ? g->p.tp + (1.0 - g->p.tp) * std::exp(-timt / g->p.tc) : g->p.tp;
 }
-
-struct Timer {
-    r3d_gpu* g;
-    bool on;
-    r3d_timing* tm;
-    std::vector<std::pair<int, int>> spans;  // (event index, category)
-    int next = 0;
-    cudaEvent_t at(int idx) {
-        while ((int)g->ev.size() <= idx) {
-            cudaEvent_t e;
-            cuda_ok(cudaEventCreate(&e), "cudaEventCreate");
-            g->ev.push_back(e);
-        }
-        return g->ev[idx];
-    }
-    void begin() {
-        if (on) cuda_ok(cudaEventRecord(at(next), g->stream), "cudaEventRecord");
-    }
-    void end(int cat) {
-        if (!on) return;
-        cuda_ok(cudaEventRecord(at(next + 1), g->stream), "cudaEventRecord");
-        spans.push_back({next, cat});
-        next += 2;
-    }
-};
 
 void launch_dt_full_any(r3d_gpu* g) {
     if (g->fp32)
@@ -440,7 +375,7 @@ void upload_background(r3d_gpu* g, const r3d_host_state* st) {
     g->bg.kf = reinterpret_cast<const float4*>(df + 2 * pad);
 }
 
-}  // namespace
+}  // namespace r3dg
 
 extern "C" {
 
@@ -554,6 +489,7 @@ int r3d_gpu_destroy(r3d_gpu* g) {
     if (!g) return R3D_OK;
     DeviceGuard dg(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
+    adjoint_free(g);
     for (int b = 0; b < 2; ++b)
         for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->X[b][q]);
     for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->Z[q]);

@@ -1,0 +1,113 @@
+// r3d_gpu_impl.hpp - the device-side simulation object behind the opaque r3d_gpu handle, and
+// the helpers shared by the forward entry points (r3d_gpu.cu) and the adjoint (adjoint.cu).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "r3d_device.cuh"
+#include "r3d_error.hpp"
+#include "r3d_gpu.h"
+#include "r3d_host.hpp"
+#include "r3d_kernels.h"
+
+namespace r3dg {
+struct Adjoint;  // reverse-mode workspace, created on first use (adjoint.cu)
+}
+
+struct r3d_gpu {
+    r3d_params p;
+    r3db::Derived d;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    r3dk::Geometry geo{};
+    r3dk::Physics ph{};
+    r3dk::Lines lines{};
+    r3dk::Boundary bnd{};
+    int nfields = 5;
+    double* X[2][r3dk::kMaxFields] = {};
+    r3dk::StageMaps maps[2];  // TMA maps of X[0] and X[1] (ru rv rw ro tt)
+    r3dk::StageMaps zmaps;    // TMA maps of the FP32 accumulators Z32
+    double* Z[r3dk::kMaxFields] = {};
+    // FP32-bulk state (precision == R3D_PREC_FP32BULK): momenta and rho', T' deviations
+    bool fp32 = false;
+    float* X32[2][5] = {};
+    float* Z32[5] = {};
+    r3dk::Background bg{};
+    void* bg_buf = nullptr;
+    double* line_buf = nullptr;
+    r3dk::Scalars* dsc = nullptr;
+    r3dk::Scalars* hsc = nullptr;  // pinned mirror
+    int cur = 0;
+    int kchunk = 32;
+    bool uploaded = false;
+    int64_t bytes = 0;
+    double host_timc = 0.0, host_timi = 0.0;  // host clock for the plume relaxation (tc != 0)
+    std::vector<cudaEvent_t> ev;             // timing events (r3d_gpu_run_timed)
+    r3dg::Adjoint* adj = nullptr;            // reverse-mode workspace (adjoint entry points)
+};
+
+namespace r3dg {
+
+inline void cuda_ok(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw r3db::Error(e == cudaErrorMemoryAllocation ? R3D_ENOMEM : R3D_ECUDA,
+                          std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
+};
+
+// CUDA-event spans of a queued step sequence (inactive when on == false).
+struct Timer {
+    r3d_gpu* g;
+    bool on;
+    r3d_timing* tm;
+    std::vector<std::pair<int, int>> spans;  // (event index, category)
+    int next = 0;
+    cudaEvent_t at(int idx) {
+        while ((int)g->ev.size() <= idx) {
+            cudaEvent_t e;
+            cuda_ok(cudaEventCreate(&e), "cudaEventCreate");
+            g->ev.push_back(e);
+        }
+        return g->ev[idx];
+    }
+    void begin() {
+        if (on) cuda_ok(cudaEventRecord(at(next), g->stream), "cudaEventRecord");
+    }
+    void end(int cat) {
+        if (!on) return;
+        cuda_ok(cudaEventRecord(at(next + 1), g->stream), "cudaEventRecord");
+        spans.push_back({next, cat});
+        next += 2;
+    }
+};
+
+// 3D TMA map over one padded field: dims (nx, ny, nz), one (box_x, box_y, 1) box per copy.
+CUtensorMap field_map(void* base, int64_t nx, int64_t ny, int64_t nz, int64_t pitch, int64_t plane,
+                      cuuint32_t box_x, cuuint32_t box_y, CUtensorMapDataType type, size_t esize);
+r3dk::FieldSet fieldset(const r3d_gpu* g);
+void launch_dt_full_any(r3d_gpu* g);
+void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_launches);
+void pull_scalars(r3d_gpu* g, r3d_scalars* sc);
+
+// adjoint.cu
+void adjoint_free(r3d_gpu* g);
+
+}  // namespace r3dg

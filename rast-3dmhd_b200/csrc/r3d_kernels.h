@@ -14,6 +14,7 @@ struct FieldSet {
     const double* xin[kMaxFields];
     double* xout[kMaxFields];
     double* z[kMaxFields];
+    double* f[kMaxFields];  // right-hand sides F, stored only by the adjoint's recompute launches
 };
 
 // FP32-bulk field pointers: thermodynamic deviations and momenta stored as float.
@@ -62,7 +63,7 @@ size_t stage_fp64_smem();
 void stage_fp64_box(unsigned* bx, unsigned* by);
 cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
                               const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
-                              int kchunk, cudaStream_t st);
+                              int kchunk, cudaStream_t st, bool emit_rhs = false);
 cudaError_t launch_bcon(const Geometry& g, const Physics& ph, const Lines& L, const Boundary& b,
                         const FieldSet& fs, Scalars* sc, int with_dt, cudaStream_t st);
 cudaError_t launch_dt_full(const Geometry& g, const Physics& ph, const Lines& L,

@@ -69,7 +69,7 @@ void stage_fp64_box(unsigned* bx, unsigned* by) {
     *by = SY;
 }
 
-template <int STAGE, bool KC, bool MHD>
+template <int STAGE, bool KC, bool MHD, bool EMIT>
 __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
     stage_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
                FieldSet fs, Scalars* sc, int kchunk) {
@@ -441,6 +441,7 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 xn[f] = zv + cg * F[f];
                 fs.xout[f][nc] = xn[f];
                 if (STAGE < 2) fs.z[f][nc] = xn[f] + cz * F[f];
+                if constexpr (EMIT) fs.f[f][nc] = F[f];  // the adjoint's recompute keeps F
             }
             if (ghost) {  // periodic images (src/communicate.cpp:108-168), edge threads only
 #pragma unroll
@@ -482,40 +483,43 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
     if (STAGE == 2) reduce_dt(der, m1, m2, m3, m4, mu, sc);
 }
 
-template <int STAGE, bool KC, bool MHD>
+template <int STAGE, bool KC, bool MHD, bool EMIT>
 static void launch_one(dim3 grid, dim3 block, const StageMaps& maps, const Geometry& g,
                        const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
                        int kchunk, cudaStream_t st) {
     static bool configured = false;
     constexpr size_t smem = Shape<MHD>::smem;
     if (!configured) {
-        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         configured = true;
     }
-    stage_fp64<STAGE, KC, MHD><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
+    stage_fp64<STAGE, KC, MHD, EMIT><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
 }
 
-template <bool MHD>
+template <bool MHD, bool EMIT>
 static void launch_stage(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                          const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
     dim3 block(TX, TY, 1);
     dim3 grid((g.npx + TX - 1) / TX, (g.npy + TY - 1) / TY, (g.npz + kchunk - 1) / kchunk);
     const bool kc = ph.kappa_const != 0;
-    if (stage == 0) kc ? launch_one<0, true, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-                       : launch_one<0, false, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
-    else if (stage == 1) kc ? launch_one<1, true, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-                            : launch_one<1, false, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
-    else kc ? launch_one<2, true, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-            : launch_one<2, false, MHD>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
+    if (stage == 0) kc ? launch_one<0, true, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
+                       : launch_one<0, false, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
+    else if (stage == 1) kc ? launch_one<1, true, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
+                            : launch_one<1, false, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
+    else kc ? launch_one<2, true, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
+            : launch_one<2, false, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
 }
 
 cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
                               const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
-                              int kchunk, cudaStream_t st) {
-    if (ph.lmag)
-        launch_stage<true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
-    else
-        launch_stage<false>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+                              int kchunk, cudaStream_t st, bool emit_rhs) {
+    if (emit_rhs) {
+        if (ph.lmag) launch_stage<true, true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+        else launch_stage<false, true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+    } else {
+        if (ph.lmag) launch_stage<true, false>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+        else launch_stage<false, false>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+    }
     return cudaGetLastError();
 }
 

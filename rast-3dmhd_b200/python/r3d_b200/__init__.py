@@ -108,6 +108,11 @@ def lib():
         L.r3d_gpu_enqueue.argtypes = [vp, ip]
         L.r3d_gpu_run_timed.argtypes = [vp, ip, ctypes.POINTER(Scalars), ctypes.POINTER(Timing)]
         L.r3d_gpu_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        dpp = ctypes.POINTER(ctypes.POINTER(ctypes.c_double))
+        L.r3d_gpu_adjoint_record.argtypes = [vp, ip, ip, ctypes.POINTER(Scalars)]
+        L.r3d_gpu_adjoint_backward.argtypes = [vp, dpp, dpp]
+        L.r3d_gpu_adjoint_step.argtypes = [vp, dpp, dpp]
+        L.r3d_gpu_adjoint_memory.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.r3d_last_error.restype = ctypes.c_char_p
         L.r3d_version.restype = ctypes.c_char_p
         _lib = L
@@ -261,6 +266,41 @@ class GpuSim:
         m, e = ctypes.c_double(), ctypes.c_double()
         _check(lib().r3d_gpu_totals(self.h, ctypes.byref(m), ctypes.byref(e)))
         return m.value, e.value
+
+    # ---- discrete adjoint (FP64) ----
+    def _fields(self):
+        return FIELDS3D if self.p.lmag else FIELDS3D[:5]
+
+    def _adjoint_call(self, fn, seed: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+        NX, NY, NZ = dims(self.p)
+        names = self._fields()
+        dp = ctypes.POINTER(ctypes.c_double)
+        src = [np.ascontiguousarray(seed[n], dtype=np.float64).reshape(NZ, NY, NX) for n in names]
+        out = {n: np.zeros((NZ, NY, NX)) for n in names}
+        sp = (dp * len(names))(*[a.ctypes.data_as(dp) for a in src])
+        gp = (dp * len(names))(*[out[n].ctypes.data_as(dp) for n in names])
+        _check(fn(self.h, sp, gp))
+        return out
+
+    def adjoint_record(self, nsteps: int, checkpoint_every: int) -> Dict[str, float]:
+        """Run nsteps forward (as run()) keeping a checkpoint every checkpoint_every steps."""
+        sc = Scalars()
+        _check(lib().r3d_gpu_adjoint_record(self.h, nsteps, checkpoint_every, ctypes.byref(sc)))
+        return sc.as_dict()
+
+    def adjoint_backward(self, seed: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+        """Cotangent of the recorded start state from the cotangent of the recorded final state."""
+        return self._adjoint_call(lib().r3d_gpu_adjoint_backward, seed)
+
+    def adjoint_step(self, seed: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+        """One-step vector-Jacobian product at the current state (the state is not advanced)."""
+        return self._adjoint_call(lib().r3d_gpu_adjoint_step, seed)
+
+    @property
+    def adjoint_memory_bytes(self) -> int:
+        b = ctypes.c_int64()
+        _check(lib().r3d_gpu_adjoint_memory(self.h, ctypes.byref(b)))
+        return int(b.value)
 
     @property
     def stream(self) -> int:
