@@ -227,6 +227,41 @@ def side_run(R, flags, steps, warmup, bytes_per_cell, fp64_ms_per_step):
     return out
 
 
+def adjoint_run(R, local):
+    """Wall time of the discrete adjoint on the MHD 64x64x128 case: record 200 steps with a
+    checkpoint every 20, then the checkpointed reverse sweep (seed: d(kinetic energy)/dX)."""
+    import numpy as np
+
+    p = R.parse(["--npx", "64", "--npy", "64", "--npz", "128", "--lmag", "1", "--beta", "10", "--rm", "1",
+                 "--ampb", "0.1", "--bfh", "2", "--bzp", "20", "--seed", "5", "--gpu", str(local)])
+    st = R.HostState.setup(p)
+    with R.GpuSim(p) as sim:
+        sim.upload(st)
+        sim.adjoint_record(20, 20)  # warm-up (allocates the workspace)
+        sim.upload(st)
+        t0 = time.perf_counter()
+        sim.adjoint_record(200, 20)
+        t1 = time.perf_counter()
+        fin = st.copy()
+        sim.download(fin)
+        seed = {n: np.zeros_like(a) for n, a in fin.fields.items()}
+        ro = fin.fields["ro"]
+        for n in ("ru", "rv", "rw"):
+            seed[n] = fin.fields[n] / ro
+        seed["ro"] = -0.5 * (fin.fields["ru"] ** 2 + fin.fields["rv"] ** 2 + fin.fields["rw"] ** 2) / ro ** 2
+        t2 = time.perf_counter()
+        sim.adjoint_backward(seed)
+        t3 = time.perf_counter()
+        mem = sim.adjoint_memory_bytes
+    cells = 64 * 64 * 128
+    return {"grid": [64, 64, 128], "steps": 200, "checkpoint_every": 20,
+            "forward_record_ms": (t1 - t0) * 1e3, "backward_ms": (t3 - t2) * 1e3,
+            "backward_over_forward": (t3 - t2) / (t1 - t0),
+            "adjoint_mcell_steps_per_s": cells * 200 / (t3 - t2) / 1e6, "adjoint_device_bytes": mem,
+            "note": "wall clock around synchronous C ABI calls (host seed upload and gradient download "
+                    "included in backward_ms)"}
+
+
 def run_reference_arm(args, world, rank, pg):
     if rank != 0:
         return 0
@@ -357,6 +392,7 @@ def main():
                                                      "--beta", "10", "--rm", "1", "--ampb", "0.1", "--bfh", "2",
                                                      "--bzp", "20", "--seed", "7", "--gpu", str(local)],
                                                  max(args.steps, 20), args.warmup, 640.0, None)
+        extra["adjoint_mhd_64x64x128"] = adjoint_run(R, local)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu = cpu_reference_sample()

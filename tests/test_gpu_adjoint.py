@@ -177,7 +177,11 @@ def test_adjoint_kinetic_energy_gradient_vs_central_differences():
         J0 = energy(0.0)
         assert J0 == pytest.approx(float(J.detach()), rel=1e-13)  # the recorded run is the plain run
         rng = np.random.default_rng(2024)
-        eps = 1e-5
+        # The directional derivative along a unit direction is ~1e-4 of J, so the rounding noise of
+        # J (~1e-14 relative after 200 steps) divided by eps dominates the difference below
+        # eps ~ 1e-4, and the O(eps^2) truncation error above ~3e-3; eps = 1e-3 sits between
+        # (differences agree with the adjoint to ~1e-8 there).
+        eps = 1e-3
         worst = 0.0
         dirs = []
         for _ in range(8):
