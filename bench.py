@@ -227,6 +227,41 @@ def side_run(R, flags, steps, warmup, bytes_per_cell, fp64_ms_per_step):
     return out
 
 
+def fp32_error_run(R, local, grid, steps, flags=()):
+    """FP32-bulk against FP64 after `steps` steps from the same initial state: per-field
+    relative L2 / Linf error on the interior, total mass and energy drift of both, and the step
+    time of both (CUDA events)."""
+    import numpy as np
+
+    base = ["--npx", str(grid[0]), "--npy", str(grid[1]), "--npz", str(grid[2]), "--seed", str(SEED),
+            "--gpu", str(local)] + list(flags)
+    out = {"grid": list(grid), "steps": steps, "flags": list(flags)}
+    states, totals, times = {}, {}, {}
+    for prec in ("fp64", "fp32bulk"):
+        p = R.parse(base + ["--precision", prec])
+        st = R.HostState.setup(p)
+        with R.GpuSim(p) as sim:
+            sim.upload(st)
+            m0, e0 = sim.totals()
+            _, tm = sim.run_timed(steps)
+            m1, e1 = sim.totals()
+            sim.download(st)
+        states[prec] = st.fields
+        totals[prec] = {"mass_drift": (m1 - m0) / m0, "energy_drift": (e1 - e0) / e0}
+        times[prec] = tm["total_ms"] / steps
+    inner = (slice(1, -1), slice(1, -1), slice(1, -1))
+    err = {}
+    for n in ("ru", "rv", "rw", "ro", "tt"):
+        a = states["fp64"][n][inner]
+        b = states["fp32bulk"][n][inner]
+        d = b - a
+        err[n] = {"rel_l2": float(np.sqrt(np.sum(d * d)) / np.sqrt(np.sum(a * a))),
+                  "rel_linf": float(np.max(np.abs(d)) / np.max(np.abs(a)))}
+    out.update({"error": err, "totals": totals, "ms_per_step": times,
+                "speedup": times["fp64"] / times["fp32bulk"]})
+    return out
+
+
 def adjoint_run(R, local):
     """Wall time of the discrete adjoint on the MHD 64x64x128 case: record 200 steps with a
     checkpoint every 20, then the checkpointed reverse sweep (seed: d(kinetic energy)/dX)."""
@@ -311,7 +346,22 @@ def main():
                     help="another grid (small cases for profiling); the default is the benchmark grid")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32bulk"],
                     help="form of the headline run (fp64 is the benchmark; fp32bulk for profiling)")
+    ap.add_argument("--fp32-error", type=int, nargs=4, metavar=("NPX", "NPY", "NPZ", "STEPS"),
+                    help="only measure FP32-bulk against FP64 on this grid after STEPS steps and print it")
+    ap.add_argument("--plume", action="store_true",
+                    help="with --fp32-error: plume forcing tp=2 tc=0 xp=yp=10 zp=0 hh=1, seed 11")
     args = ap.parse_args()
+    if args.fp32_error:
+        import r3d_b200 as R
+
+        global SEED
+        fl = []
+        if args.plume:
+            SEED = 11
+            fl = ["--tp", "2", "--tc", "0", "--xp", "10", "--yp", "10", "--zp", "0", "--hh", "1"]
+        g = args.fp32_error
+        print(json.dumps(fp32_error_run(R, 0, g[:3], g[3], fl)))
+        return 0
     global GRID, FLAGS
     if args.grid:
         GRID = tuple(args.grid)
@@ -393,6 +443,7 @@ def main():
                                                      "--bzp", "20", "--seed", "7", "--gpu", str(local)],
                                                  max(args.steps, 20), args.warmup, 640.0, None)
         extra["adjoint_mhd_64x64x128"] = adjoint_run(R, local)
+        extra["fp32bulk_error_504x504x512_100steps"] = fp32_error_run(R, local, GRID, 100)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu = cpu_reference_sample()
