@@ -475,6 +475,11 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
             g->kchunk = R3D_KCHUNK;
 #else
             g->kchunk = p->npz >= 512 ? 64 : (p->npz >= 256 ? 32 : 16);
+            if (p->lmag) {
+                // one CTA per SM: prefer enough z-chunks for >= 8 full waves over 148 SMs
+                const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + 7) / 8);
+                while (g->kchunk > 16 && tiles * ((p->npz + g->kchunk - 1) / g->kchunk) < 8 * 148) g->kchunk /= 2;
+            }
 #endif
             cuda_ok(cudaStreamSynchronize(g->stream), "create");
         } catch (...) {
