@@ -11,8 +11,9 @@ dataset exists for this path); the working set (15 x 1.07 GB) is far larger than
 Timing: W untimed steps, then K steps timed with CUDA events recorded by the library on the
 stream its kernels run on (every launch is bracketed, which also yields the per-kernel
 durations for the roofline); barrier + device synchronise on both sides; max over ranks.
-Under torchrun each rank runs its own replica of the workload (the single-GPU form keeps the
-whole domain on one device; slab decomposition over GPUs is not part of this build).
+Under torchrun (N > 1) the domain grows to 504 x 504 x (512 N) and each rank holds one
+504 x 504 x 512 z slab on its GPU (weak scaling): the ghost planes move over NCCL after every
+stage and the dt limits are all-reduced on the device every step, inside the timed region.
 The reference arm (--impl reference) times the reference's own CPU sources (compiled
 unmodified into oracle/_ref) on a bounded slab of the same workload, on rank 0 only.
 """
@@ -379,12 +380,25 @@ def main():
 
     import r3d_b200 as R
 
-    p = R.parse(FLAGS + ["--seed", str(SEED), "--gpu", str(local), "--precision", args.precision])
-    cells = GRID[0] * GRID[1] * GRID[2]
     fp32 = args.precision == "fp32bulk"
     bytes_step = 200.0 if fp32 else BYTES_PER_CELL_STEP
-    st = R.HostState.setup(p)
-    sim = R.GpuSim(p)
+    if world == 1:
+        p = R.parse(FLAGS + ["--seed", str(SEED), "--gpu", str(local), "--precision", args.precision])
+        cells = GRID[0] * GRID[1] * GRID[2]
+        st = R.HostState.setup(p)
+        sim = R.GpuSim(p)
+    else:
+        # weak scaling: the domain is npx x npy x (npz * N), one z slab of npz planes per GPU,
+        # ghost planes exchanged over NCCL after every stage, dt limits all-reduced per step
+        from r3d_b200 import dist as D
+
+        p = R.parse(["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(GRID[2] * world),
+                     "--seed", str(SEED), "--gpu", str(local), "--precision", args.precision])
+        z0, nz = D.slab_of(p.npz, rank, world)
+        cells = GRID[0] * GRID[1] * nz
+        st = R.HostState.setup_slab(p, z0, nz)
+        sim = R.GpuSim(p, slab=(z0, nz))
+        sim.halo_init(D.share_unique_id(rank, pg), rank, world)
     sim.upload(st)
     with ClockSampler(local) as clk:
         sim.run(args.warmup)                     # untimed warm-up
@@ -434,7 +448,7 @@ def main():
 
     sim.close()
     extra = {}
-    if not args.no_extra and not args.grid and not fp32:
+    if not args.no_extra and not args.grid and not fp32 and world == 1:
         extra["fp32bulk_504x504x512"] = side_run(R, FLAGS + ["--seed", str(SEED), "--precision", "fp32bulk",
                                                              "--gpu", str(local)], args.steps, args.warmup,
                                                  200.0, ms_per_step)
@@ -456,7 +470,9 @@ def main():
                                       f"polytrope + RAN2 seed {SEED} ampt 0.005",
                           "grid": list(GRID), "precision": args.precision, "bit_exact": not fp32,
                           "l2": "inputs 16 GB >> 126 MB L2 (no flush needed)",
-                          "parallelism": f"{world} replica(s), one GPU each"},
+                          "parallelism": ("1 GPU" if world == 1 else
+                                          f"{world} z-slabs of {GRID[0]}x{GRID[1]}x{GRID[2]}, one per GPU "
+                                          f"(NCCL ghost planes per stage, dt all-reduce per step)")},
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": int(tm["total_launches"]), "clocks": clk.summary(),
                "final_dt": sc["dt"], "extra": extra}

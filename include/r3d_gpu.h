@@ -96,15 +96,50 @@ int r3d_dims(const r3d_params* p, int64_t* nx, int64_t* ny, int64_t* nz);
 /* ---- host set-up: grid metrics + conductivity + static IC + ghost fill (src/main.cpp:134-154,
  *      src/grid.cpp:148-284, src/static_ic.cpp:24-161, src/ode.cpp:152-174) ---------------- */
 int r3d_setup_host(const r3d_params* p, r3d_host_state* st, r3d_scalars* sc);
+/* The same for the z slab of r3d_gpu_create_slab: fields hold global planes z0 .. z0+nz+1 and
+ * the z metric lines nz+2 entries from global index z0 (x/y lines in full); identical to the
+ * corresponding part of r3d_setup_host (the RAN2 stream is advanced past the planes above). */
+int r3d_setup_host_slab(const r3d_params* p, int z0, int nz, r3d_host_state* st, r3d_scalars* sc);
 /* Static polytrope T(k), R(k), k = 0..npz-1 (src/ode.cpp:152-174). */
 int r3d_static_profile(const r3d_params* p, double* t, double* r);
 
 /* ---- device state (replaces gpu_alloc / gpu_upload / gpu_download / gpu_free,
  *      include/gpu.hpp:35-38) ----------------------------------------------------------- */
 int r3d_gpu_create(const r3d_params* p, r3d_gpu** out);
+/* A handle over the z slab of global planes z0+1 .. z0+nz (4 <= nz; the reference's npez
+ * decomposition, src/topology.cpp): its host arrays hold nz+2 planes, global planes z0 .. z0+nz+1,
+ * the outer two being the z neighbours' planes (or the domain's ghost planes); the z metric
+ * lines are the global ones from index z0 on.  BCON and the one-sided edge stencils apply only
+ * where the slab touches the domain's top or bottom.  On its own a slab handle sees its ghost
+ * planes as constants; r3d_gpu_halo_init connects the slabs of several processes. */
+int r3d_gpu_create_slab(const r3d_params* p, int z0, int nz, r3d_gpu** out);
 int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc);
 int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc);
 int r3d_gpu_destroy(r3d_gpu* g);
+/* ---- z slabs over several processes (replaces the MPI/NCCL halo exchange of
+ *      src/communicate.cpp:70-182 and the dt MPI_Allreduce of src/step.cpp:224) ----
+ * One process per GPU, rank r holding the r-th slab in z order.  Rank 0 calls
+ * r3d_nccl_unique_id and distributes the 128 bytes; every rank then calls r3d_gpu_halo_init
+ * (collective).  From then on every step combines the dt limits of all slabs (ncclAllReduce on
+ * the device) and exchanges the ghost planes after every stage (ncclSend/ncclRecv), all on the
+ * library stream; results equal the single-domain run bit for bit.  NCCL is loaded at run time
+ * (libnccl.so.2); R3D_EINVAL when it is absent. */
+int r3d_nccl_unique_id(unsigned char* out, size_t len);
+int r3d_gpu_halo_init(r3d_gpu* g, const unsigned char* id, size_t len, int rank, int nranks);
+
+/* ---- the same decomposition inside one process (several slabs on one device) ----
+ * nslabs slabs of npz/nslabs (+1) planes on device gpu_id, exchanging ghost planes by device
+ * copies; upload/step/run/download take the global host state like r3d_gpu_*.  Needs tc == 0
+ * when tp != 0 (one shared host clock is not kept). */
+typedef struct r3d_mesh r3d_mesh;
+int r3d_mesh_create(const r3d_params* p, int nslabs, r3d_mesh** out);
+int r3d_mesh_slab(const r3d_mesh* m, int r, int* z0, int* nz);
+int r3d_mesh_upload(r3d_mesh* m, const r3d_host_state* st, const r3d_scalars* sc);
+int r3d_mesh_step(r3d_mesh* m, int nstages, r3d_scalars* sc);
+int r3d_mesh_run(r3d_mesh* m, int nsteps, r3d_scalars* sc);
+int r3d_mesh_download(r3d_mesh* m, r3d_host_state* st, r3d_scalars* sc);
+int r3d_mesh_destroy(r3d_mesh* m);
+
 /* Bytes of device memory held by g. */
 int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes);
 /* The CUDA stream (cudaStream_t) every kernel of g is launched on. */

@@ -20,7 +20,7 @@ HOST_SRCS = ["host/params.cpp", "host/setup.cpp"]
 # FMA contraction: off everywhere the FP64 result must equal the reference CPU build; on for
 # the FP32-bulk kernels, which carry no bit-exactness contract.
 FMAD_ON = {"csrc/step_fp32.cu", "csrc/bcon_fp32.cu"}
-CU_SRCS = ["csrc/step_fp64.cu", "csrc/bcon.cu", "csrc/step_fp32.cu", "csrc/bcon_fp32.cu", "csrc/r3d_gpu.cu", "csrc/dt_noalloc.cu", "csrc/adjoint.cu"]
+CU_SRCS = ["csrc/step_fp64.cu", "csrc/bcon.cu", "csrc/step_fp32.cu", "csrc/bcon_fp32.cu", "csrc/r3d_gpu.cu", "csrc/dt_noalloc.cu", "csrc/adjoint.cu", "csrc/halo.cu", "csrc/mesh.cu"]
 LIB = os.path.join(PKG, "lib", "librast3d_b200.so")
 BIN = os.path.join(PKG, "bin", "r3d_b200")
 
@@ -57,7 +57,7 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
             fmad = ["-fmad=true"] if s in FMAD_ON else ["-fmad=false"]
             _run([NVCC] + ARCH + COMMON + fmad + extra + lang + ["-c", src, "-o", obj])
     if force or _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs + ["-cudart", "static"])
+        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs + ["-cudart", "static", "-ldl"])
     main = os.path.join(PKG, "host", "r3d_main.cpp")
     if os.path.exists(main) and (force or _stale(BIN, [main, LIB])):
         _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),

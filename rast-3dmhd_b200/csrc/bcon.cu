@@ -30,8 +30,9 @@ __global__ void __launch_bounds__(256) bcon_kernel(Geometry g, Physics ph, Lines
         double* tt = fs.xout[4];
         const double c13 = ph.c13, c23 = ph.c23, c43 = ph.c43;
         const int64_t P = g.plane, row = (int64_t)j * g.pitch + i;
-        // top, k = 1 (src/bcon.cpp:27-98)
-        {
+        // top, k = 1 (src/bcon.cpp:27-98); a z slab that does not hold the domain's top
+        // plane has a neighbour's ghost plane there instead
+        if (g.top_edge) {
             const int64_t n = P + row;
             const double ro1 = ro[n], ro2 = ro[n + P], ro3 = ro[n + 2 * P];
             const double u = ro1 * (c43 * ru[n + P] / ro2 - c13 * ru[n + 2 * P] / ro3);
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(256) bcon_kernel(Geometry g, Physics ph, Lines
             }
         }
         // bottom, k = npz (src/bcon.cpp:104-139)
-        {
+        if (g.bot_edge) {
             const int64_t n = (int64_t)g.npz * P + row;
             const double ro1 = ro[n], ro2 = ro[n - P], ro3 = ro[n - 2 * P];
             const double u = ro1 * (c43 * ru[n - P] / ro2 - c13 * ru[n - 2 * P] / ro3);

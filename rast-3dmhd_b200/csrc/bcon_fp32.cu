@@ -28,6 +28,7 @@ __global__ void __launch_bounds__(256) bcon_fp32_kernel(Geometry g, Physics ph, 
         const double c13 = ph.c13, c23 = ph.c23, c43 = ph.c43;
         const int64_t P = g.plane, row = (int64_t)j * g.pitch + i;
         for (int side = 0; side < 2; ++side) {
+            if (side == 0 ? !g.top_edge : !g.bot_edge) continue;  // slab interior face
             const int k = side == 0 ? 1 : g.npz;
             const int dk = side == 0 ? 1 : -1;
             const int64_t n = (int64_t)k * P + row, n1 = n + dk * P, n2 = n + 2 * dk * P;

@@ -16,9 +16,11 @@ constexpr int kMaxFields = 8;  // ru rv rw ro tt bx by bz
 // Everything a stage kernel needs besides the field pointers.  Host-computed products keep
 // the reference association (e.g. tmpy[j] = hy*dyydy[j], src/fluxes.cpp:90).
 struct Geometry {
-    int npx, npy, npz;
-    int64_t pitch;  // doubles per row
-    int64_t plane;  // doubles per z plane
+    int npx, npy, npz;  // npz: planes held by this device (a z slab of the domain, or all of it)
+    int64_t pitch;      // doubles per row
+    int64_t plane;      // doubles per z plane
+    int top_edge;       // local plane 1 is the domain's top plane (BCON, one-sided stencils)
+    int bot_edge;       // local plane npz is the domain's bottom plane
 };
 
 struct Physics {

@@ -132,15 +132,18 @@ r3dk::FieldSet32 fieldset32(const r3d_gpu* g) {
 }
 
 // R(k), T0(k) over the global z index: ghost 0 -> T(0), interior k -> T(k-1), ghost npz+1 -> the
-// bottom value (src/static_ic.cpp:53-89 stitched over ranks).
-void background_columns(const r3d_params& p, std::vector<double>& R, std::vector<double>& T) {
+// bottom value (src/static_ic.cpp:53-89 stitched over ranks); for a z slab, the nloc+2 planes
+// from global plane z0 on.
+void background_columns(const r3d_gpu* g, std::vector<double>& R, std::vector<double>& T) {
+    const r3d_params& p = g->p;
     std::vector<double> t, r;
     static_profile(p, t, r);
-    const int nz = p.npz + 2;
-    R.assign(nz, 0.0);
-    T.assign(nz, 0.0);
-    for (int k = 0; k < nz; ++k) {
-        const int src = k == 0 ? 0 : (k == nz - 1 ? p.npz - 1 : k - 1);
+    const int nz = p.npz + 2, nl = g->nloc + 2;
+    R.assign(nl, 0.0);
+    T.assign(nl, 0.0);
+    for (int k = 0; k < nl; ++k) {
+        const int kg = g->z0 + k;
+        const int src = kg == 0 ? 0 : (kg == nz - 1 ? p.npz - 1 : kg - 1);
         R[k] = r[src];
         T[k] = t[src];
     }
@@ -159,9 +162,40 @@ void launch_dt_full_any(r3d_gpu* g) {
 }
 
 // Queue one step (nstages substages) on the device.
+void enqueue_step_begin(r3d_gpu* g) {
+    g->bnd.tpr = plume_tpr(g);
+    if (g->halo) halo_reduce_limits(g);
+    cuda_ok(r3dk::launch_step_begin(g->ph, g->dsc, g->stream), "step_begin");
+}
+
+void enqueue_stage(r3d_gpu* g, int s) {
+    if (g->fp32) {
+        r3dk::FieldSet32 fs = fieldset32(g);
+        cuda_ok(r3dk::launch_stage_fp32(s, g->maps[g->cur], g->zmaps, g->geo, g->ph, g->lines, g->bg, fs, g->dsc,
+                                        g->kchunk, g->stream),
+                "stage32");
+        cuda_ok(r3dk::launch_bcon_fp32(g->geo, g->ph, g->lines, g->bnd, g->bg, fs, g->dsc, s == 2 ? 1 : 0, g->stream),
+                "bcon32");
+    } else {
+        FieldSet fs = fieldset(g);
+        cuda_ok(r3dk::launch_stage_fp64(s, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream),
+                "stage");
+        cuda_ok(r3dk::launch_bcon(g->geo, g->ph, g->lines, g->bnd, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon");
+    }
+    g->cur = 1 - g->cur;
+}
+
+void enqueue_step_end(r3d_gpu* g, int nstages) {
+    cuda_ok(r3dk::launch_step_end(g->dsc, g->stream), "step_end");
+    if (nstages < 3) launch_dt_full_any(g);  // the next dt needs the limits of this partial-step state
+}
+
+// Queue one step (nstages substages) on the device; with a Halo, the dt keys are reduced over
+// the slabs before the step and the ghost planes exchanged after every stage.
 void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_launches) {
     g->bnd.tpr = plume_tpr(g);
     tm.begin();
+    if (g->halo) halo_reduce_limits(g);
     cuda_ok(r3dk::launch_step_begin(g->ph, g->dsc, g->stream), "step_begin");
     tm.end(2);
     ++launches;
@@ -184,6 +218,11 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
         launches += 2;
         ++stage_launches;
         g->cur = 1 - g->cur;
+        if (g->halo) {
+            tm.begin();
+            halo_exchange(g);
+            tm.end(2);
+        }
     }
     tm.begin();
     cuda_ok(r3dk::launch_step_end(g->dsc, g->stream), "step_end");
@@ -194,6 +233,17 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
     }
     tm.end(2);
 }
+
+void* state_field(r3d_gpu* g, int q, size_t* esize) {
+    if (g->fp32) {
+        *esize = sizeof(float);
+        return g->X32[g->cur][q];
+    }
+    *esize = sizeof(double);
+    return g->X[g->cur][q];
+}
+
+int state_fields(const r3d_gpu* g) { return g->fp32 ? 5 : g->nfields; }
 
 void pull_scalars(r3d_gpu* g, r3d_scalars* sc) {
     cuda_ok(cudaMemcpyAsync(g->hsc, g->dsc, sizeof(r3dk::Scalars), cudaMemcpyDeviceToHost, g->stream),
@@ -312,7 +362,7 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
     g->ph.kappa_const = kc ? 1 : 0;
     const double dzs = (double)(1.0f / (float)(p.npz - 1));
     g->bnd.dz_top = dzs / st->dzzdz[1];            // src/bcon.cpp:59
-    g->bnd.dz_bot = dzs / st->dzzdz[p.npz];        // src/bcon.cpp:124
+    g->bnd.dz_bot = dzs / st->dzzdz[NZ - 2];       // src/bcon.cpp:124 (plane npz of the domain)
 }
 
 // FP32-bulk background tables (see r3dk::Background).
@@ -321,7 +371,7 @@ void upload_background(r3d_gpu* g, const r3d_host_state* st) {
     const Derived& d = g->d;
     const int64_t NZ = d.nz;
     std::vector<double> R, T;
-    background_columns(p, R, T);
+    background_columns(g, R, T);
     std::vector<double> hres(NZ, 0.0), dt0(NZ, 0.0), lt0(NZ, 0.0);
     for (int64_t k = 1; k < NZ - 1; ++k) {
         const double tz = d.hz * st->dzzdz[k];
@@ -377,28 +427,42 @@ void upload_background(r3d_gpu* g, const r3d_host_state* st) {
 
 }  // namespace r3dg
 
-extern "C" {
+namespace r3dg {
 
-int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
-    return guarded([&] {
-        if (!p || !out) throw std::invalid_argument("null argument");
-        *out = nullptr;
-        check_params(*p);
-        auto g = new r3d_gpu();
-        try {
+// A handle over global planes z0+1 .. z0+nloc (the whole domain: z0 = 0, nloc = npz); its host
+// and device arrays hold nloc+2 planes, the outer two being the z neighbours' planes (or the
+// domain's constant ghost planes).  With shared_stream the handle launches on that stream and
+// does not own it.
+r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t shared_stream) {
+    const r3d_params* p = &pin;
+    check_params(*p);
+    if (z0 < 0 || nloc < 4 || z0 + nloc > p->npz)
+        throw std::invalid_argument("a z slab needs 4 <= nloc and z0 + nloc <= npz");
+    auto g = new r3d_gpu();
+    try {
             g->p = *p;
             g->d = derive(*p);
+            g->z0 = z0;
+            g->nloc = nloc;
+            g->d.nz = nloc + 2;  // planes held here (global extents stay in p)
             g->device = p->gpu_id;
             int ndev = 0;
             cuda_ok(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
             if (g->device < 0 || g->device >= ndev) throw std::invalid_argument("--gpu id out of range");
             DeviceGuard dg(g->device);
-            cuda_ok(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            if (shared_stream) {
+                g->stream = shared_stream;
+                g->own_stream = false;
+            } else {
+                cuda_ok(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            }
             const Derived& d = g->d;
             g->nfields = p->lmag ? 8 : 5;
             g->geo.npx = p->npx;
             g->geo.npy = p->npy;
-            g->geo.npz = p->npz;
+            g->geo.npz = nloc;
+            g->geo.top_edge = z0 == 0 ? 1 : 0;
+            g->geo.bot_edge = z0 + nloc == p->npz ? 1 : 0;
             g->geo.pitch = (d.nx + 15) / 16 * 16;
             g->geo.plane = g->geo.pitch * d.ny;
             if (g->geo.plane * d.nz >= (int64_t(1) << 31))
@@ -474,26 +538,26 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
             #ifdef R3D_KCHUNK
             g->kchunk = R3D_KCHUNK;
 #else
-            g->kchunk = p->npz >= 512 ? 64 : (p->npz >= 256 ? 32 : 16);
+            g->kchunk = nloc >= 512 ? 64 : (nloc >= 256 ? 32 : 16);
             if (p->lmag) {
                 // one CTA per SM: prefer enough z-chunks for >= 8 full waves over 148 SMs
                 const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + 7) / 8);
-                while (g->kchunk > 16 && tiles * ((p->npz + g->kchunk - 1) / g->kchunk) < 8 * 148) g->kchunk /= 2;
+                while (g->kchunk > 16 && tiles * ((nloc + g->kchunk - 1) / g->kchunk) < 8 * 148) g->kchunk /= 2;
             }
 #endif
             cuda_ok(cudaStreamSynchronize(g->stream), "create");
-        } catch (...) {
-            r3d_gpu_destroy(g);
-            throw;
-        }
-        *out = g;
-    });
+    } catch (...) {
+        destroy_handle(g);
+        throw;
+    }
+    return g;
 }
 
-int r3d_gpu_destroy(r3d_gpu* g) {
-    if (!g) return R3D_OK;
+void destroy_handle(r3d_gpu* g) {
+    if (!g) return;
     DeviceGuard dg(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
+    halo_free(g);
     adjoint_free(g);
     for (int b = 0; b < 2; ++b)
         for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->X[b][q]);
@@ -506,8 +570,32 @@ int r3d_gpu_destroy(r3d_gpu* g) {
     cudaFree(g->dsc);
     if (g->hsc) cudaFreeHost(g->hsc);
     for (auto e : g->ev) cudaEventDestroy(e);
-    if (g->stream) cudaStreamDestroy(g->stream);
+    if (g->stream && g->own_stream) cudaStreamDestroy(g->stream);
     delete g;
+}
+
+}  // namespace r3dg
+
+extern "C" {
+
+int r3d_gpu_create(const r3d_params* p, r3d_gpu** out) {
+    return guarded([&] {
+        if (!p || !out) throw std::invalid_argument("null argument");
+        *out = nullptr;
+        *out = create_handle(*p, 0, p->npz, nullptr);
+    });
+}
+
+int r3d_gpu_create_slab(const r3d_params* p, int z0, int nz, r3d_gpu** out) {
+    return guarded([&] {
+        if (!p || !out) throw std::invalid_argument("null argument");
+        *out = nullptr;
+        *out = create_handle(*p, z0, nz, nullptr);
+    });
+}
+
+int r3d_gpu_destroy(r3d_gpu* g) {
+    destroy_handle(g);
     return R3D_OK;
 }
 
@@ -527,7 +615,7 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
         if (g->fp32) {
             upload_background(g, st);
             std::vector<double> R, T;
-            background_columns(g->p, R, T);
+            background_columns(g, R, T);
             const int64_t NX = d.nx, NY = d.ny, NZ = d.nz, per = NX * NY;
             std::vector<float> tmp((size_t)(per * NZ));
             for (int q = 0; q < 5; ++q) {
@@ -575,7 +663,7 @@ int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc) {
         double* dst[r3dk::kMaxFields] = {st->ru, st->rv, st->rw, st->ro, st->tt, st->bx, st->by, st->bz};
         if (g->fp32) {
             std::vector<double> R, T;
-            background_columns(g->p, R, T);
+            background_columns(g, R, T);
             const int64_t NX = d.nx, NY = d.ny, NZ = d.nz, per = NX * NY;
             std::vector<float> tmp((size_t)(per * NZ));
             cuda_ok(cudaStreamSynchronize(g->stream), "download");

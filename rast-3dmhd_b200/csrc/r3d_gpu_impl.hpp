@@ -18,6 +18,7 @@
 
 namespace r3dg {
 struct Adjoint;  // reverse-mode workspace, created on first use (adjoint.cu)
+struct Halo;     // inter-process slab exchange (halo.cu)
 }
 
 struct r3d_gpu {
@@ -50,6 +51,10 @@ struct r3d_gpu {
     double host_timc = 0.0, host_timi = 0.0;  // host clock for the plume relaxation (tc != 0)
     std::vector<cudaEvent_t> ev;             // timing events (r3d_gpu_run_timed)
     r3dg::Adjoint* adj = nullptr;            // reverse-mode workspace (adjoint entry points)
+    // z slab held by this handle: global planes z0+1 .. z0+nloc (the whole domain: 0, npz)
+    int z0 = 0, nloc = 0;
+    bool own_stream = true;
+    r3dg::Halo* halo = nullptr;              // ghost-plane exchange with other slabs (NCCL)
 };
 
 namespace r3dg {
@@ -106,6 +111,22 @@ r3dk::FieldSet fieldset(const r3d_gpu* g);
 void launch_dt_full_any(r3d_gpu* g);
 void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_launches);
 void pull_scalars(r3d_gpu* g, r3d_scalars* sc);
+
+// Slab handles (a z range of the domain) and the pieces of one step, for drivers that
+// interleave several slabs with their ghost-plane exchanges (mesh.cu, halo.cu).
+r3d_gpu* create_handle(const r3d_params& p, int z0, int nloc, cudaStream_t shared_stream);
+void destroy_handle(r3d_gpu* g);
+void enqueue_step_begin(r3d_gpu* g);
+void enqueue_stage(r3d_gpu* g, int s);  // stage s + BCON; the new state becomes current
+void enqueue_step_end(r3d_gpu* g, int nstages);
+// Device pointer and element size of field q of the current state (FP64 or FP32-bulk).
+void* state_field(r3d_gpu* g, int q, size_t* esize);
+int state_fields(const r3d_gpu* g);
+
+// halo.cu
+void halo_free(r3d_gpu* g);
+void halo_reduce_limits(r3d_gpu* g);  // before step_begin: global min/max of the dt keys
+void halo_exchange(r3d_gpu* g);       // after a stage: ghost planes from the z neighbours
 
 // adjoint.cu
 void adjoint_free(r3d_gpu* g);

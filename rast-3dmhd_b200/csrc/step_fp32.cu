@@ -196,15 +196,15 @@ __global__ void __launch_bounds__(NT, 3)
 #define DV_(P, F, DX, DY) P[(F)*SN + s0 + (DY)*SX + (DX)]
         const float4 ka = bg.kf[3 * k], kb4 = bg.kf[3 * k + 1], kc4 = bg.kf[3 * k + 2];
         const float cz0 = ka.x;
-        const bool edge = (k == 1) || (k == g.npz);
+        const bool edge = (k == 1 && g.top_edge) || (k == g.npz && g.bot_edge);
 
         // continuity (momenta only, no background)
         float fr = (RW_(r0, R_RU, -1, 0) - RW_(r0, R_RU, 1, 0)) * cx;
         fr -= (RW_(r0, R_RV, 0, 1) - RW_(r0, R_RV, 0, -1)) * cy;
         float dwz;
-        if (k == 1)
+        if (k == 1 && g.top_edge)
             dwz = (4.0f * RW_(rp, R_RW, 0, 0) - fs.xin[R_RW][nc + 2 * PL]) * cz0;
-        else if (k == g.npz)
+        else if (k == g.npz && g.bot_edge)
             dwz = (fs.xin[R_RW][nc - 2 * PL] - 4.0f * RW_(rm, R_RW, 0, 0)) * cz0;
         else
             dwz = (RW_(rp, R_RW, 0, 0) - RW_(rm, R_RW, 0, 0)) * cz0;

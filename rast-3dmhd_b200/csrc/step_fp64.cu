@@ -188,15 +188,15 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
 #define RW_(P, F, DX, DY) P[(F)*RAWF + s0 + (DY)*SX + (DX)]
 #define DV_(P, F, DX, DY) P[(F)*SN + s0 + (DY)*SX + (DX)]
             const double tmpz = L.tmpz[k];
-            const bool edge = (k == 1) || (k == g.npz);
+            const bool edge = (k == 1 && g.top_edge) || (k == g.npz && g.bot_edge);
 
             // ---- continuity, src/fluxes.cpp:87-121 ----
             double fr = (RW_(r0, R_RU, -1, 0) - RW_(r0, R_RU, 1, 0)) * hx * dx1;
             fr -= (RW_(r0, R_RV, 0, 1) - RW_(r0, R_RV, 0, -1)) * tmpy;
             double dwz;
-            if (k == 1)
+            if (k == 1 && g.top_edge)
                 dwz = (4.0 * RW_(rp, R_RW, 0, 0) - fs.xin[R_RW][nc + 2 * PL]) * tmpz;
-            else if (k == g.npz)
+            else if (k == g.npz && g.bot_edge)
                 dwz = (fs.xin[R_RW][nc - 2 * PL] - 4.0 * RW_(rm, R_RW, 0, 0)) * tmpz;
             else
                 dwz = (RW_(rp, R_RW, 0, 0) - RW_(rm, R_RW, 0, 0)) * tmpz;
@@ -340,11 +340,11 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 const double BZzp = RW_(rp, R_BZ, 0, 0), BZzm = RW_(rm, R_BZ, 0, 0);
                 // dW/dz with the one-sided forms at the top and bottom planes (2245-2259)
                 double wzb = wz;
-                if (k == 1) {
+                if (k == 1 && g.top_edge) {
                     const int n2 = nc + 2 * PL;
                     const double w2 = fs.xin[R_RW][n2] * __drcp_rn(fs.xin[R_RO][n2]);
                     wzb = (4.0 * Wzp - w2) * hz * dzk;
-                } else if (k == g.npz) {
+                } else if (k == g.npz && g.bot_edge) {
                     const int n2 = nc - 2 * PL;
                     const double w2 = fs.xin[R_RW][n2] * __drcp_rn(fs.xin[R_RO][n2]);
                     wzb = (w2 - 4.0 * Wzm) * hz * dzk;
@@ -381,14 +381,14 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 b1 = b1 - W0 * bxz;                        // 1370
                 b2f = b2f - V0 * byy;                      // 1380
                 double d2bxz, d2byz;
-                if (k == 1) {  // 1391, 1511
+                if (k == 1 && g.top_edge) {  // 1391, 1511
                     const double bx2 = fs.xin[R_BX][nc + 2 * PL], bx3 = fs.xin[R_BX][nc + 3 * PL];
                     const double by2 = fs.xin[R_BY][nc + 2 * PL], by3 = fs.xin[R_BY][nc + 3 * PL];
                     d2bxz = (-3.0 * BX0 + 4.0 * BXzp - bx2) * hz * d2z +
                             (2.0 * BX0 - 5.0 * BXzp + 4.0 * bx2 - bx3) * h2z * dzk * dzk;
                     d2byz = (-3.0 * BY0 + 4.0 * BYzp - by2) * hz * d2z +
                             (2.0 * BY0 - 5.0 * BYzp + 4.0 * by2 - by3) * h2z * dzk * dzk;
-                } else if (k == g.npz) {  // 1392, 1513
+                } else if (k == g.npz && g.bot_edge) {  // 1392, 1513
                     const double bx2 = fs.xin[R_BX][nc - 2 * PL], bx3 = fs.xin[R_BX][nc - 3 * PL];
                     const double by2 = fs.xin[R_BY][nc - 2 * PL], by3 = fs.xin[R_BY][nc - 3 * PL];
                     d2bxz = (3.0 * BX0 - 4.0 * BXzm + bx2) * hz * d2z +

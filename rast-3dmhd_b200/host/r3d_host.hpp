@@ -63,7 +63,7 @@ void static_profile(const r3d_params& p, std::vector<double>& t, std::vector<dou
 
 // Fill st (arrays sized by the caller) with metrics, conductivity, the static IC, the seeded
 // temperature perturbation and the periodic ghosts; returns tb in sc.
-void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc);
+void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc, int z0, int nz);
 
 // Periodic x/y ghost copy of one field over every z plane (src/communicate.cpp:70-168 on one
 // domain: y rows first, then x columns).

@@ -11,6 +11,7 @@
 //    x fastest) order (src/static_ic.cpp:122-153); because ranks own contiguous z and y
 //    ranges this is the global (k, j, i) order for every decomposition.
 // Arithmetic (association, single-precision seeds, libm calls) matches the reference.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -318,10 +319,14 @@ void fill_ghosts(double* f, int64_t nx, int64_t ny, int64_t nz) {
     }
 }
 
-void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc) {
+// The initial state on global planes z0 .. z0+nz+1 (the whole domain: z0 = 0, nz = npz); the z
+// metric lines are written from global index z0 on, nz+2 entries.
+void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc, int z0, int nz) {
     check_params(p);
+    if (z0 < 0 || nz < 1 || z0 + nz > p.npz) throw std::invalid_argument("z range outside the domain");
     const Derived d = derive(p);
-    const int64_t NX = d.nx, NY = d.ny, NZ = d.nz, N = NX * NY * NZ;
+    const int64_t NX = d.nx, NY = d.ny, NZ = (int64_t)nz + 2, N = NX * NY * NZ;
+    const int64_t NZG = d.nz;  // global planes (with the two ghost planes)
     auto need = [](const double* a, const char* n) {
         if (!a) throw std::invalid_argument(std::string("r3d_host_state.") + n + " is NULL");
     };
@@ -333,8 +338,11 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc)
     };
     put(st.exx, m.x.s); put(st.dxxdx, m.x.d1); put(st.d2xxdx2, m.x.d2); put(st.ddx, m.x.dd);
     put(st.wyy, m.y.s); put(st.dyydy, m.y.d1); put(st.d2yydy2, m.y.d2); put(st.ddy, m.y.dd);
-    put(st.zee, m.z.s); put(st.dzzdz, m.z.d1); put(st.d2zzdz2, m.z.d2); put(st.ddz, m.z.dd);
-    put(st.rkapa, m.rkapa); put(st.dkapa, m.dkapa);
+    auto putz = [&](double* dst, const std::vector<double>& v) {
+        if (dst) std::memcpy(dst, v.data() + z0, sizeof(double) * (size_t)NZ);
+    };
+    putz(st.zee, m.z.s); putz(st.dzzdz, m.z.d1); putz(st.d2zzdz2, m.z.d2); putz(st.ddz, m.z.dd);
+    putz(st.rkapa, m.rkapa); putz(st.dkapa, m.dkapa);
 
     for (double* a : {st.ru, st.rv, st.rw, st.ro, st.tt}) std::memset(a, 0, sizeof(double) * N);
     if (p.lmag)
@@ -346,8 +354,9 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc)
     auto at = [&](int64_t i, int64_t j, int64_t k) { return i + NX * (j + NY * k); };
     // columns (src/static_ic.cpp:53-89): ghost top = T(0), interior k = T(k-1), ghost bottom = tb
     for (int64_t k = 0; k < NZ; ++k) {
-        const double tv = k == 0 ? T[0] : (k == NZ - 1 ? tb : T[k - 1]);
-        const double rv = k == 0 ? R[0] : (k == NZ - 1 ? rb : R[k - 1]);
+        const int64_t kg = z0 + k;
+        const double tv = kg == 0 ? T[0] : (kg == NZG - 1 ? tb : T[kg - 1]);
+        const double rv = kg == 0 ? R[0] : (kg == NZG - 1 ? rb : R[kg - 1]);
         for (int64_t j = 1; j <= NY - 2; ++j)
             for (int64_t i = 1; i <= NX - 2; ++i) {
                 st.tt[at(i, j, k)] = tv;
@@ -357,27 +366,37 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc)
     if (p.lmag) {
         // magnetic layer (src/static_ic.cpp:94-108)
         const double cln = widen(-4.0f * logf(2.0f)) / (p.bfh * p.bfh);
-        for (int64_t k = 1; k <= NZ - 2; ++k) {
-            const double z = m.z.s[k];
+        for (int64_t k = 0; k < NZ; ++k) {
+            const int64_t kg = z0 + k;
+            if (kg < 1 || kg > NZG - 2) continue;
+            const double z = m.z.s[kg];
             const double bfac = p.ampb * std::exp(cln * (z - p.bzp) * (z - p.bzp));
             for (int64_t n = at(0, 0, k); n < at(0, 0, k + 1); ++n) st.bx[n] = bfac;
         }
-        for (int64_t k = 1; k <= NZ - 2; ++k)
+        for (int64_t k = 0; k < NZ; ++k) {
+            const int64_t kg = z0 + k;
+            if (kg < 1 || kg > NZG - 2) continue;
             for (int64_t j = 1; j <= NY - 2; ++j)
                 for (int64_t i = 1; i <= NX - 2; ++i) {
                     const int64_t n = at(i, j, k);
                     st.ro[n] = st.ro[n] - st.bx[n] * st.bx[n] / st.tt[n] * d.obeta;
                 }
+        }
     }
     if (p.ampt != 0.0) {
         // temperature perturbation (src/static_ic.cpp:114-159), global (k, j, i) draw order
+        // a slab skips the draws of the interior planes above it
         Ran2 rng(-p.seed);
-        for (int64_t k = 1; k <= NZ - 2; ++k)
+        const int64_t kfirst = std::max<int64_t>(1, z0), klast = std::min<int64_t>(NZG - 2, z0 + NZ - 1);
+        for (int64_t n = 0; n < (kfirst - 1) * (NX - 2) * (NY - 2); ++n) rng.next();
+        for (int64_t kg = kfirst; kg <= klast; ++kg) {
+            const int64_t k = kg - z0;
             for (int64_t j = 1; j <= NY - 2; ++j)
                 for (int64_t i = 1; i <= NX - 2; ++i) {
                     const double w = 1.0 + p.ampt * (rng.next() - 0.5);
                     st.tt[at(i, j, k)] *= w;
                 }
+        }
     }
     for (double* a : {st.ru, st.rv, st.rw, st.tt, st.ro}) fill_ghosts(a, NX, NY, NZ);
     if (p.lmag)
@@ -400,7 +419,14 @@ extern "C" {
 int r3d_setup_host(const r3d_params* p, r3d_host_state* st, r3d_scalars* sc) {
     return guarded([&] {
         if (!p || !st || !sc) throw std::invalid_argument("null argument");
-        setup_state(*p, *st, *sc);
+        setup_state(*p, *st, *sc, 0, p->npz);
+    });
+}
+
+int r3d_setup_host_slab(const r3d_params* p, int z0, int nz, r3d_host_state* st, r3d_scalars* sc) {
+    return guarded([&] {
+        if (!p || !st || !sc) throw std::invalid_argument("null argument");
+        setup_state(*p, *st, *sc, z0, nz);
     });
 }
 

@@ -108,6 +108,18 @@ def lib():
         L.r3d_gpu_enqueue.argtypes = [vp, ip]
         L.r3d_gpu_run_timed.argtypes = [vp, ip, ctypes.POINTER(Scalars), ctypes.POINTER(Timing)]
         L.r3d_gpu_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.r3d_setup_host_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(_HostStateC),
+                                          ctypes.POINTER(Scalars)]
+        L.r3d_gpu_create_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(vp)]
+        L.r3d_nccl_unique_id.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        L.r3d_gpu_halo_init.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ip, ip]
+        L.r3d_mesh_create.argtypes = [ctypes.POINTER(Params), ip, ctypes.POINTER(vp)]
+        L.r3d_mesh_slab.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.r3d_mesh_upload.argtypes = [vp, ctypes.POINTER(_HostStateC), ctypes.POINTER(Scalars)]
+        L.r3d_mesh_step.argtypes = [vp, ip, ctypes.POINTER(Scalars)]
+        L.r3d_mesh_run.argtypes = [vp, ip, ctypes.POINTER(Scalars)]
+        L.r3d_mesh_download.argtypes = [vp, ctypes.POINTER(_HostStateC), ctypes.POINTER(Scalars)]
+        L.r3d_mesh_destroy.argtypes = [vp]
         dpp = ctypes.POINTER(ctypes.POINTER(ctypes.c_double))
         L.r3d_gpu_adjoint_record.argtypes = [vp, ip, ip, ctypes.POINTER(Scalars)]
         L.r3d_gpu_adjoint_backward.argtypes = [vp, dpp, dpp]
@@ -179,6 +191,34 @@ class HostState:
         return cls(fields, lines, {})
 
     @classmethod
+    def empty_slab(cls, p: Params, nz: int) -> "HostState":
+        """Arrays for the z slab of nz planes: nz+2 planes, z lines of nz+2 entries."""
+        NX, NY, _ = dims(p)
+        names = FIELDS3D if p.lmag else FIELDS3D[:5]
+        fields = {n: np.zeros((nz + 2, NY, NX)) for n in names}
+        lines = {}
+        for q, n in enumerate(LINES):
+            lines[n] = np.zeros(NX if q < 4 else (NY if q < 8 else nz + 2))
+        return cls(fields, lines, {})
+
+    @classmethod
+    def setup_slab(cls, p: Params, z0: int, nz: int) -> "HostState":
+        """The initial state on global planes z0 .. z0+nz+1 (r3d_setup_host_slab)."""
+        st = cls.empty_slab(p, nz)
+        sc = Scalars()
+        c = st._c()
+        _check(lib().r3d_setup_host_slab(ctypes.byref(p), z0, nz, ctypes.byref(c), ctypes.byref(sc)))
+        st.scalars = sc.as_dict()
+        return st
+
+    def slab_view(self, z0: int, nz: int) -> "HostState":
+        """Views (no copy) of this global state on planes z0 .. z0+nz+1."""
+        f = {n: a[z0:z0 + nz + 2] for n, a in self.fields.items()}
+        ln = {n: (a[z0:z0 + nz + 2] if q >= 8 else a) for q, (n, a) in enumerate(
+            (m, self.lines[m]) for m in LINES)}
+        return HostState(f, ln, dict(self.scalars))
+
+    @classmethod
     def setup(cls, p: Params) -> "HostState":
         """Grid metrics, conductivity, static IC, seeded perturbation, periodic ghosts."""
         st = cls.empty(p)
@@ -209,11 +249,20 @@ class HostState:
 class GpuSim:
     """Device-resident simulation (replaces GpuSim + gpu_alloc/upload/step_gpu/download/free)."""
 
-    def __init__(self, p: Params):
+    def __init__(self, p: Params, slab=None):
+        """slab=(z0, nz): a handle over global planes z0+1 .. z0+nz (r3d_gpu_create_slab)."""
         self.p = p
+        self.slab = slab
         h = ctypes.c_void_p()
-        _check(lib().r3d_gpu_create(ctypes.byref(p), ctypes.byref(h)))
+        if slab is None:
+            _check(lib().r3d_gpu_create(ctypes.byref(p), ctypes.byref(h)))
+        else:
+            _check(lib().r3d_gpu_create_slab(ctypes.byref(p), int(slab[0]), int(slab[1]), ctypes.byref(h)))
         self.h = h
+
+    def halo_init(self, unique_id: bytes, rank: int, nranks: int):
+        """Join the NCCL slab exchange (collective over the nranks processes)."""
+        _check(lib().r3d_gpu_halo_init(self.h, unique_id, len(unique_id), rank, nranks))
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
@@ -311,6 +360,68 @@ class GpuSim:
         b = ctypes.c_int64()
         _check(lib().r3d_gpu_memory(self.h, ctypes.byref(b)))
         return int(b.value)
+
+
+def nccl_unique_id() -> bytes:
+    """128-byte NCCL id for r3d_gpu_halo_init (rank 0 makes it, every rank receives it)."""
+    buf = ctypes.create_string_buffer(128)
+    _check(lib().r3d_nccl_unique_id(buf, 128))
+    return buf.raw
+
+
+class GpuMesh:
+    """The z-slab decomposition inside one process (r3d_mesh_*): nslabs slabs on one device."""
+
+    def __init__(self, p: Params, nslabs: int):
+        self.p = p
+        h = ctypes.c_void_p()
+        _check(lib().r3d_mesh_create(ctypes.byref(p), nslabs, ctypes.byref(h)))
+        self.h = h
+        self.nslabs = nslabs
+
+    def slab(self, r: int):
+        z0, nz = ctypes.c_int(), ctypes.c_int()
+        _check(lib().r3d_mesh_slab(self.h, r, ctypes.byref(z0), ctypes.byref(nz)))
+        return z0.value, nz.value
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().r3d_mesh_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, st: HostState):
+        sc = Scalars(**{k: (int(v) if k == "nit" else v) for k, v in st.scalars.items()})
+        c = st._c()
+        _check(lib().r3d_mesh_upload(self.h, ctypes.byref(c), ctypes.byref(sc)))
+
+    def step(self, nstages: int = 3) -> Dict[str, float]:
+        sc = Scalars()
+        _check(lib().r3d_mesh_step(self.h, nstages, ctypes.byref(sc)))
+        return sc.as_dict()
+
+    def run(self, nsteps: int) -> Dict[str, float]:
+        sc = Scalars()
+        _check(lib().r3d_mesh_run(self.h, nsteps, ctypes.byref(sc)))
+        return sc.as_dict()
+
+    def download(self, st: HostState) -> Dict[str, float]:
+        sc = Scalars()
+        c = st._c()
+        _check(lib().r3d_mesh_download(self.h, ctypes.byref(c), ctypes.byref(sc)))
+        st.scalars = sc.as_dict()
+        return st.scalars
 
 
 def version() -> str:

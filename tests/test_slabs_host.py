@@ -1,0 +1,78 @@
+"""Host side of the z-slab decomposition: slab set-up, partition, and the NCCL id hand-out over
+a two-process gloo group (no GPU needed)."""
+import os
+
+import numpy as np
+import pytest
+
+import r3d_b200 as R
+from r3d_b200 import dist as D
+
+MAG = ["--lmag", "1", "--beta", "10", "--rm", "1", "--ampb", "0.1", "--bfh", "2", "--bzp", "20"]
+
+
+@pytest.mark.parametrize("mhd", [False, True], ids=["hydro", "mhd"])
+def test_setup_slab_equals_global_slices(mhd):
+    p = R.parse(["--npx", "12", "--npy", "10", "--npz", "24", "--seed", "5"] + (MAG if mhd else []))
+    g = R.HostState.setup(p)
+    for z0, nz in ((0, 6), (6, 7), (13, 11), (0, 24), (5, 19)):
+        sl = R.HostState.setup_slab(p, z0, nz)
+        v = g.slab_view(z0, nz)
+        for n in sl.fields:
+            assert np.array_equal(sl.fields[n], v.fields[n]), (z0, nz, n)
+        for n in sl.lines:
+            assert np.array_equal(sl.lines[n], v.lines[n]), (z0, nz, n)
+        assert sl.scalars == g.scalars
+
+
+def test_slab_partition():
+    for npz in (8, 24, 37, 512):
+        for n in (1, 2, 3, 4):
+            if npz // n < 4:
+                with pytest.raises(ValueError):
+                    D.slab_of(npz, 0, n)
+                continue
+            parts = [D.slab_of(npz, r, n) for r in range(n)]
+            assert parts[0][0] == 0 and sum(nz for _, nz in parts) == npz
+            for (a, na), (b, _) in zip(parts, parts[1:]):
+                assert a + na == b
+    with pytest.raises(R.R3dError):
+        R.HostState.setup_slab(R.parse(["--npx", "8", "--npy", "8", "--npz", "8"]), 6, 4)
+
+
+def _rank(rank, world, port, q):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        uid = D.share_unique_id(rank, dist, make=lambda: bytes(range(128)))
+        z0, nz = D.slab_of(40, rank, world)
+        q.put((rank, uid, z0, nz))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_unique_id_broadcast_two_ranks():
+    import multiprocessing as mp
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    out = sorted(q.get(timeout=120) for _ in range(2))
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    assert out[0][1] == out[1][1] == bytes(range(128))
+    assert (out[0][2], out[0][3], out[1][2], out[1][3]) == (0, 20, 20, 20)
+
+
+def test_nccl_unique_id_is_128_bytes():
+    uid = R.nccl_unique_id()
+    assert isinstance(uid, bytes) and len(uid) == 128
