@@ -322,6 +322,8 @@ class GpuSim:
 
     def _adjoint_call(self, fn, seed: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
         NX, NY, NZ = dims(self.p)
+        if self.slab is not None:
+            NZ = self.slab[1] + 2
         names = self._fields()
         dp = ctypes.POINTER(ctypes.c_double)
         src = [np.ascontiguousarray(seed[n], dtype=np.float64).reshape(NZ, NY, NX) for n in names]
