@@ -140,6 +140,12 @@ int r3d_mesh_run(r3d_mesh* m, int nsteps, r3d_scalars* sc);
 int r3d_mesh_download(r3d_mesh* m, r3d_host_state* st, r3d_scalars* sc);
 int r3d_mesh_destroy(r3d_mesh* m);
 
+/* Test hook for the failure path: from the next step on, every TMA transaction of the stage
+ * kernels expects `bytes` more than its copies deliver, so each bounded wait runs out (200 ms),
+ * the kernel records the error and returns, and the step reports R3D_ECUDA; the context stays
+ * usable.  0 (the default, restored by r3d_gpu_upload) switches it off. */
+int r3d_gpu_debug_tma_extra(r3d_gpu* g, unsigned int bytes);
+
 /* Bytes of device memory held by g. */
 int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes);
 /* The CUDA stream (cudaStream_t) every kernel of g is launched on. */

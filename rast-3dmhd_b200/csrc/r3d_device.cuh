@@ -63,6 +63,9 @@ struct Scalars {
     double dt, timc, timt, timi, umach, tb;
     int nit;
     int err;  // nonzero: a kernel gave up on a bounded wait (code = kernel id)
+    // Test hook (r3d_gpu_debug_tma_extra): bytes added to every expected TMA transaction of the
+    // stage kernels, so that their bounded waits run out; 0 in every normal run.
+    unsigned int tx_extra;
     unsigned long long wmin[4];  // keys of min(ww1), min(ww2), min(ww3), min(vv)
     unsigned long long umax;     // key of max(ogamma*uu/tt)
     double mass, energy;         // diagnostics (r3d_gpu_totals)

@@ -690,6 +690,16 @@ int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc) {
     });
 }
 
+int r3d_gpu_debug_tma_extra(r3d_gpu* g, unsigned int bytes) {
+    return guarded([&] {
+        if (!g) throw std::invalid_argument("null handle");
+        DeviceGuard dg(g->device);
+        cuda_ok(cudaMemcpyAsync(&g->dsc->tx_extra, &bytes, sizeof bytes, cudaMemcpyHostToDevice, g->stream),
+                "tx_extra");
+        cuda_ok(cudaStreamSynchronize(g->stream), "tx_extra");
+    });
+}
+
 int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes) {
     if (!g || !bytes) return R3D_EINVAL;
     *bytes = g->bytes;

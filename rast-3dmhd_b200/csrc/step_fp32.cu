@@ -86,12 +86,13 @@ __global__ void __launch_bounds__(NT, 3)
     int zlast_issued = kb - 1, zlast_waited = kb - 1;
     // Z (the RK accumulator, stored one column left-shifted so interior boxes start 16-byte
     // aligned) of plane p, no halo, into a 3-slot ring; slot (p-kb)%3, phase ((p-kb)/3)&1
+    unsigned int tx_extra = 0;  // read by thread 0 (test hook, normally 0)
     auto zissue = [&](int p) {
         zlast_issued = p;
         const int q = p - kb;
         uint64_t* bar = &zbars[q % NZS];
         float* dst = zsm + (q % NZS) * Z_SLOT;
-        mbar_expect_tx(bar, kZTx);
+        mbar_expect_tx(bar, kZTx + tx_extra);
 #pragma unroll
         for (int f = 0; f < 5; ++f) tma_load_3d(dst + f * ZF, &zmaps.m[f], bar, i0 - 1, j0, p);
     };
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(NT, 3)
         const int q = p - (kb - 1);
         uint64_t* bar = &bars[q % NRAW];
         float* dst = raw + (q % NRAW) * RAW_SLOT;
-        mbar_expect_tx(bar, kPlaneTx);
+        mbar_expect_tx(bar, kPlaneTx + tx_extra);
 #pragma unroll
         for (int f = 0; f < R_NF; ++f) tma_load_3d(dst + f * RAWF, &maps.m[f], bar, i0 - 1, j0 - 1, p);
     };
@@ -135,6 +136,7 @@ __global__ void __launch_bounds__(NT, 3)
 
     if (tid == 0) {
         s_abort = (*(volatile int*)&sc->err != kErrNone) ? 2 : 0;
+        tx_extra = sc->tx_extra;
         for (int b = 0; b < NRAW + NZS; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
     }

@@ -91,12 +91,13 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
 
     // plane p has local index q = p - (kb - 1); ring slot q % 4, mbarrier phase (q / 4) & 1
     int last_issued = kb - 2, last_waited = kb - 2;  // bookkeeping of thread 0 for the drain
+    unsigned int tx_extra = 0;                          // read by thread 0 (test hook, normally 0)
     auto issue = [&](int p) {
         last_issued = p;
         const int q = p - (kb - 1);
         uint64_t* bar = &bars[q % NRAW];
         double* dst = raw + (q % NRAW) * S::raw_slot;
-        mbar_expect_tx(bar, S::plane_tx);
+        mbar_expect_tx(bar, S::plane_tx + tx_extra);
 #pragma unroll
         for (int f = 0; f < NF; ++f) tma_load_3d(dst + f * RAWF, &maps.m[f], bar, i0 - 1, j0 - 1, p);
     };
@@ -121,6 +122,7 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
     if (tid == 0) {
         // a CTA that finds an earlier timeout recorded leaves before issuing any copy
         s_abort = (*(volatile int*)&sc->err != kErrNone) ? 2 : 0;
+        tx_extra = sc->tx_extra;
         for (int b = 0; b < NRAW; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
     }

@@ -108,6 +108,7 @@ def lib():
         L.r3d_gpu_enqueue.argtypes = [vp, ip]
         L.r3d_gpu_run_timed.argtypes = [vp, ip, ctypes.POINTER(Scalars), ctypes.POINTER(Timing)]
         L.r3d_gpu_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.r3d_gpu_debug_tma_extra.argtypes = [vp, ctypes.c_uint]
         L.r3d_setup_host_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(_HostStateC),
                                           ctypes.POINTER(Scalars)]
         L.r3d_gpu_create_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(vp)]
@@ -315,6 +316,10 @@ class GpuSim:
         m, e = ctypes.c_double(), ctypes.c_double()
         _check(lib().r3d_gpu_totals(self.h, ctypes.byref(m), ctypes.byref(e)))
         return m.value, e.value
+
+    def debug_tma_extra(self, nbytes: int):
+        """Test hook: make the stage kernels' bounded TMA waits run out (0 switches it off)."""
+        _check(lib().r3d_gpu_debug_tma_extra(self.h, nbytes))
 
     # ---- discrete adjoint (FP64) ----
     def _fields(self):
