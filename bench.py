@@ -347,6 +347,10 @@ def main():
                     help="another grid (small cases for profiling); the default is the benchmark grid")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32bulk"],
                     help="form of the headline run (fp64 is the benchmark; fp32bulk for profiling)")
+    ap.add_argument("--slabs", action="store_true",
+                    help="run a single GPU through the NCCL z-slab path (one rank), as N > 1 does")
+    ap.add_argument("--mhd", action="store_true",
+                    help="MHD (--lmag 1 --beta 10 --rm 1, layer ampb 0.1 bfh 2 bzp 20; for profiling cases)")
     ap.add_argument("--fp32-error", type=int, nargs=4, metavar=("NPX", "NPY", "NPZ", "STEPS"),
                     help="only measure FP32-bulk against FP64 on this grid after STEPS steps and print it")
     ap.add_argument("--plume", action="store_true",
@@ -382,8 +386,12 @@ def main():
 
     fp32 = args.precision == "fp32bulk"
     bytes_step = 200.0 if fp32 else BYTES_PER_CELL_STEP
-    if world == 1:
-        p = R.parse(FLAGS + ["--seed", str(SEED), "--gpu", str(local), "--precision", args.precision])
+    mag = (["--lmag", "1", "--beta", "10", "--rm", "1", "--ampb", "0.1", "--bfh", "2", "--bzp", "20"]
+           if args.mhd else [])
+    if args.mhd:
+        bytes_step = 640.0
+    if world == 1 and not args.slabs:
+        p = R.parse(FLAGS + mag + ["--seed", str(SEED), "--gpu", str(local), "--precision", args.precision])
         cells = GRID[0] * GRID[1] * GRID[2]
         st = R.HostState.setup(p)
         sim = R.GpuSim(p)
@@ -393,7 +401,7 @@ def main():
         from r3d_b200 import dist as D
 
         p = R.parse(["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(GRID[2] * world),
-                     "--seed", str(SEED), "--gpu", str(local), "--precision", args.precision])
+                     "--seed", str(SEED), "--gpu", str(local), "--precision", args.precision] + mag)
         z0, nz = D.slab_of(p.npz, rank, world)
         cells = GRID[0] * GRID[1] * nz
         st = R.HostState.setup_slab(p, z0, nz)
@@ -440,7 +448,7 @@ def main():
     peak, peak_kind = peak_hbm()
     alg_bytes_launch = cells * bytes_step / 3.0
     achieved = alg_bytes_launch / (stage_avg_ms / 1e3) / 1e9
-    traffic = None if fp32 else stage_traffic_per_launch(cells)
+    traffic = None if (fp32 or args.mhd) else stage_traffic_per_launch(cells)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
                 "kernel": ("stage_fp32" if fp32 else "stage_fp64") + " (fused FLUXES + RK3 stage update)",
@@ -448,7 +456,7 @@ def main():
 
     sim.close()
     extra = {}
-    if not args.no_extra and not args.grid and not fp32 and world == 1:
+    if not args.no_extra and not args.grid and not fp32 and world == 1 and not args.slabs and not args.mhd:
         extra["fp32bulk_504x504x512"] = side_run(R, FLAGS + ["--seed", str(SEED), "--precision", "fp32bulk",
                                                              "--gpu", str(local)], args.steps, args.warmup,
                                                  200.0, ms_per_step)
@@ -466,11 +474,11 @@ def main():
                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if fp32 else "f64",
                "data": "synthetic",
-               "config": {"workload": f"{'FP32-bulk' if fp32 else 'FP64'} hydro {GRID[0]}x{GRID[1]}x{GRID[2]}, default physics, "
+               "config": {"workload": f"{'FP32-bulk' if fp32 else 'FP64'} {'MHD' if args.mhd else 'hydro'} {GRID[0]}x{GRID[1]}x{GRID[2]}, default physics, "
                                       f"polytrope + RAN2 seed {SEED} ampt 0.005",
                           "grid": list(GRID), "precision": args.precision, "bit_exact": not fp32,
                           "l2": "inputs 16 GB >> 126 MB L2 (no flush needed)",
-                          "parallelism": ("1 GPU" if world == 1 else
+                          "parallelism": ("1 GPU" if world == 1 and not args.slabs else
                                           f"{world} z-slabs of {GRID[0]}x{GRID[1]}x{GRID[2]}, one per GPU "
                                           f"(NCCL ghost planes per stage, dt all-reduce per step)")},
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

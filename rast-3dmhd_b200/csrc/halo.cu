@@ -12,11 +12,14 @@
 // the reduction exact and order-free, so every slab count gives the bit-identical dt of the
 // single-domain run.
 //
-// NCCL is loaded at run time (dlopen of libnccl.so.2: the copy a PyTorch process has already
-// loaded, else the system one), so the library itself has no link-time NCCL dependency.
+// NCCL is loaded at run time, so the library itself has no link-time NCCL dependency: an NCCL
+// the process has already loaded (a PyTorch process has its own) is used as it is; otherwise
+// $R3D_NCCL_LIBRARY or libnccl.so.2 is opened with local symbol scope, so that a later import of
+// PyTorch still binds to its own NCCL.
 #include <dlfcn.h>
 #include <nccl.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -49,8 +52,11 @@ namespace {
 Nccl& nccl() {
     static Nccl n;
     if (n.dl) return n;
-    void* dl = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
-    if (!dl) dl = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+    void* dl = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    if (!dl) {
+        const char* path = std::getenv("R3D_NCCL_LIBRARY");
+        dl = dlopen(path && *path ? path : "libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+    }
     if (!dl) throw Error(R3D_EINVAL, std::string("NCCL is not available: ") + dlerror());
     auto sym = [&](const char* name) {
         void* f = dlsym(dl, name);

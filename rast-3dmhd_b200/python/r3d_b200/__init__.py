@@ -263,6 +263,7 @@ class GpuSim:
 
     def halo_init(self, unique_id: bytes, rank: int, nranks: int):
         """Join the NCCL slab exchange (collective over the nranks processes)."""
+        _prefer_torch_nccl()
         _check(lib().r3d_gpu_halo_init(self.h, unique_id, len(unique_id), rank, nranks))
 
     def close(self):
@@ -369,8 +370,18 @@ class GpuSim:
         return int(b.value)
 
 
+def _prefer_torch_nccl():
+    """In a process that uses PyTorch, load torch (and with it its NCCL) before the library
+    opens NCCL, so both use the same NCCL."""
+    try:
+        import torch  # noqa: F401
+    except ImportError:
+        pass
+
+
 def nccl_unique_id() -> bytes:
     """128-byte NCCL id for r3d_gpu_halo_init (rank 0 makes it, every rank receives it)."""
+    _prefer_torch_nccl()
     buf = ctypes.create_string_buffer(128)
     _check(lib().r3d_nccl_unique_id(buf, 128))
     return buf.raw
