@@ -336,6 +336,8 @@ def run_reference_arm(args, world, rank, pg):
 
 
 def main():
+    # the JSON line is the only output on stdout: NCCL's version banner stays off
+    os.environ.setdefault("NCCL_DEBUG", "WARN")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=60)
