@@ -140,6 +140,14 @@ int r3d_mesh_run(r3d_mesh* m, int nsteps, r3d_scalars* sc);
 int r3d_mesh_download(r3d_mesh* m, r3d_host_state* st, r3d_scalars* sc);
 int r3d_mesh_destroy(r3d_mesh* m);
 
+/* FLUXES (src/fluxes.cpp:44-533; with lmag the LMAG branch of 3dmhdsub.f:2146-2650) of the
+ * current device state, without changing it: out = nfields host arrays (NX*NY*NZ) receiving
+ * FU FV FW FR FT (+ the B fluxes WW1 WW2 WW3), interior cells, ghosts 0.  On the domain's top
+ * and bottom planes the momentum and energy right-hand sides, which BCON overwrites, are
+ * returned as 0; the continuity and B fluxes there are the reference's one-sided forms.
+ * FP64 only. */
+int r3d_gpu_fluxes(r3d_gpu* g, double* const* out);
+
 /* Test hook for the failure path: from the next step on, every TMA transaction of the stage
  * kernels expects `bytes` more than its copies deliver, so each bounded wait runs out (200 ms),
  * the kernel records the error and returns, and the step reports R3D_ECUDA; the context stays

@@ -559,6 +559,7 @@ void destroy_handle(r3d_gpu* g) {
     if (g->stream) cudaStreamSynchronize(g->stream);
     halo_free(g);
     adjoint_free(g);
+    cudaFree(g->fscr);
     for (int b = 0; b < 2; ++b)
         for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->X[b][q]);
     for (int q = 0; q < r3dk::kMaxFields; ++q) cudaFree(g->Z[q]);
@@ -687,6 +688,49 @@ int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc) {
             }
         }
         pull_scalars(g, sc);
+    });
+}
+
+int r3d_gpu_fluxes(r3d_gpu* g, double* const* out) {
+    return guarded([&] {
+        if (!g || !out) throw std::invalid_argument("null argument");
+        if (!g->uploaded) throw Error(R3D_ESTATE, "fluxes before upload");
+        if (g->fp32) throw Error(R3D_EINVAL, "r3d_gpu_fluxes needs precision fp64");
+        DeviceGuard dg(g->device);
+        const Derived& d = g->d;
+        const size_t fe = (size_t)g->geo.plane * d.nz;
+        const int nf = g->nfields;
+        if (!g->fscr) {
+            cuda_ok(cudaMalloc(&g->fscr, 3 * (size_t)nf * fe * sizeof(double)), "cudaMalloc(flux scratch)");
+            cuda_ok(cudaMemsetAsync(g->fscr, 0, 3 * (size_t)nf * fe * sizeof(double), g->stream), "cudaMemset");
+            g->bytes += (int64_t)(3 * (size_t)nf * fe * sizeof(double));
+        }
+        FieldSet fs{};
+        for (int q = 0; q < nf; ++q) {
+            fs.xin[q] = g->X[g->cur][q];
+            fs.xout[q] = g->fscr + (size_t)q * fe;                 // stage result, discarded
+            fs.z[q] = g->fscr + (size_t)(nf + q) * fe;             // accumulator, discarded
+            fs.f[q] = g->fscr + (size_t)(2 * nf + q) * fe;         // F
+        }
+        cuda_ok(r3dk::launch_stage_fp64(0, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk,
+                                        g->stream, true),
+                "fluxes");
+        std::vector<double> buf((size_t)(d.nx * d.ny * d.nz));
+        for (int q = 0; q < nf; ++q) {
+            if (!out[q]) throw std::invalid_argument("null output field");
+            cuda_ok(cudaMemcpy2DAsync(buf.data(), d.nx * sizeof(double), fs.f[q], g->geo.pitch * sizeof(double),
+                                      d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyDeviceToHost, g->stream),
+                    "fluxes download");
+            cuda_ok(cudaStreamSynchronize(g->stream), "fluxes");
+            for (int64_t k = 0; k < d.nz; ++k)
+                for (int64_t j = 0; j < d.ny; ++j)
+                    for (int64_t i = 0; i < d.nx; ++i) {
+                        const bool inner = k >= 1 && k <= d.nz - 2 && j >= 1 && j <= d.ny - 2 && i >= 1 && i <= d.nx - 2;
+                        const size_t n = (size_t)((k * d.ny + j) * d.nx + i);
+                        out[q][n] = inner ? buf[n] : 0.0;
+                    }
+        }
+        pull_scalars(g, nullptr);
     });
 }
 

@@ -55,6 +55,7 @@ struct r3d_gpu {
     int z0 = 0, nloc = 0;
     bool own_stream = true;
     r3dg::Halo* halo = nullptr;              // ghost-plane exchange with other slabs (NCCL)
+    double* fscr = nullptr;                  // r3d_gpu_fluxes scratch: X', Z', F (nfields each)
 };
 
 namespace r3dg {

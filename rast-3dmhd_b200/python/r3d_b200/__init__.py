@@ -109,6 +109,7 @@ def lib():
         L.r3d_gpu_run_timed.argtypes = [vp, ip, ctypes.POINTER(Scalars), ctypes.POINTER(Timing)]
         L.r3d_gpu_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.r3d_gpu_debug_tma_extra.argtypes = [vp, ctypes.c_uint]
+        L.r3d_gpu_fluxes.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
         L.r3d_setup_host_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(_HostStateC),
                                           ctypes.POINTER(Scalars)]
         L.r3d_gpu_create_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(vp)]
@@ -317,6 +318,18 @@ class GpuSim:
         m, e = ctypes.c_double(), ctypes.c_double()
         _check(lib().r3d_gpu_totals(self.h, ctypes.byref(m), ctypes.byref(e)))
         return m.value, e.value
+
+    def fluxes(self) -> Dict[str, np.ndarray]:
+        """FLUXES of the current state: fu fv fw fr ft (+ w1 w2 w3), shapes (NZ, NY, NX)."""
+        NX, NY, NZ = dims(self.p)
+        if self.slab is not None:
+            NZ = self.slab[1] + 2
+        names = ["fu", "fv", "fw", "fr", "ft"] + (["w1", "w2", "w3"] if self.p.lmag else [])
+        out = {n: np.zeros((NZ, NY, NX)) for n in names}
+        dp = ctypes.POINTER(ctypes.c_double)
+        arr = (dp * len(names))(*[out[n].ctypes.data_as(dp) for n in names])
+        _check(lib().r3d_gpu_fluxes(self.h, arr))
+        return out
 
     def debug_tma_extra(self, nbytes: int):
         """Test hook: make the stage kernels' bounded TMA waits run out (0 switches it off)."""
