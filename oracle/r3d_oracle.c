@@ -15,9 +15,11 @@
  *
  * Pinning: the hydro path is checked bit for bit against the reference CPU sources compiled
  * unmodified (oracle/_ref) and against the reference's known-answer tests
- * (tests/test_oracle_pins.py).  The MHD flux branch has no reference CPU implementation
- * (src/fluxes.cpp:539-541 aborts) and no golden data: it is "parity unpinned" beyond its
- * initial condition and dt terms, which the reference C++ does implement.
+ * (tests/test_oracle_pins.py).  The MHD flux branch has no reference C++ implementation
+ * (src/fluxes.cpp:539-541 aborts) and the Fortran cannot be compiled here; it is checked bit
+ * for bit against the reference's Fortran source executed statement by statement
+ * (oracle/fortran_lmag.py, tests/test_oracle_mhd_pin.py).  The MHD initial condition and dt
+ * terms are checked against the reference C++, which implements them.
  */
 #include "r3d_oracle.h"
 

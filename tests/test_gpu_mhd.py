@@ -4,8 +4,9 @@ The reference C++ aborts on --lmag in FLUXES (src/fluxes.cpp:539-541); the oracl
 Fortran LMAG branch (golden/fortran/3dmhdsub.f:2146-2650) on top of the pinned C++ hydro, with
 the B stage updates of 3dmhdsub.f:907-1177, Bz = 0 at the top and bottom (src/bcon.cpp:95-98,
 136-139) and the magnetic dt terms of src/step.cpp:144-156,195,213-229.  Its MHD initial
-condition is pinned to the reference build (tests/test_oracle_ref.py); the flux branch itself
-is parity-unpinned, so this test is GPU == restatement.
+condition is pinned to the reference build (tests/test_oracle_ref.py) and its LMAG fluxes to the
+reference's Fortran source executed statement by statement (tests/test_oracle_mhd_pin.py), so
+GPU == restatement is GPU == reference.
 """
 import numpy as np
 import pytest
