@@ -626,18 +626,26 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
                     float* o = tmp.data() + k * per;
                     for (int64_t n = 0; n < per; ++n) o[n] = (float)(a[n] - bgv);
                 }
-                for (int b = 0; b < 2; ++b)
-                    cuda_ok(cudaMemcpy2D(g->X32[b][q], g->geo.pitch * sizeof(float), tmp.data(),
-                                         NX * sizeof(float), NX * sizeof(float), NY * NZ, cudaMemcpyHostToDevice),
-                            "upload state32");
+                cuda_ok(cudaMemcpy2D(g->X32[0][q], g->geo.pitch * sizeof(float), tmp.data(), NX * sizeof(float),
+                                     NX * sizeof(float), NY * NZ, cudaMemcpyHostToDevice),
+                        "upload state32");
+                // the second buffer gets the same contents on the device (its z ghost planes are
+                // never written by a stage)
+                cuda_ok(cudaMemcpyAsync(g->X32[1][q], g->X32[0][q], (size_t)g->geo.plane * NZ * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, g->stream),
+                        "upload state32");
             }
         } else {
-            for (int b = 0; b < 2; ++b)
-                for (int q = 0; q < g->nfields; ++q)
-                    cuda_ok(cudaMemcpy2DAsync(g->X[b][q], g->geo.pitch * sizeof(double), src[q],
-                                              d.nx * sizeof(double), d.nx * sizeof(double), d.ny * d.nz,
-                                              cudaMemcpyHostToDevice, g->stream),
-                            "upload state");
+            for (int q = 0; q < g->nfields; ++q) {
+                cuda_ok(cudaMemcpy2DAsync(g->X[0][q], g->geo.pitch * sizeof(double), src[q], d.nx * sizeof(double),
+                                          d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyHostToDevice, g->stream),
+                        "upload state");
+                // the second buffer gets the same contents on the device (its z ghost planes are
+                // never written by a stage)
+                cuda_ok(cudaMemcpyAsync(g->X[1][q], g->X[0][q], (size_t)g->geo.plane * d.nz * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, g->stream),
+                        "upload state");
+            }
         }
         g->cur = 0;
         r3dk::Scalars h{};
