@@ -501,6 +501,7 @@ int r3d_gpu_adjoint_record(r3d_gpu* g, int nsteps, int checkpoint_every, r3d_sca
         if (!g->uploaded) throw Error(R3D_ESTATE, "record before upload");
         if (nsteps < 1 || checkpoint_every < 1) throw std::invalid_argument("nsteps and checkpoint_every must be >= 1");
         DeviceGuard dg(g->device);
+        Range r("r3d.adjoint_record");
         Adjoint* A = workspace(g);
         A->recorded = false;
         free_states(A->ckpt);
@@ -531,6 +532,7 @@ int r3d_gpu_adjoint_backward(r3d_gpu* g, const double* const* seed, double* cons
         if (!g || !seed || !grad) throw std::invalid_argument("null argument");
         if (!g->adj || !g->adj->recorded) throw Error(R3D_ESTATE, "no recorded trajectory (call r3d_gpu_adjoint_record)");
         DeviceGuard dg(g->device);
+        Range r("r3d.adjoint_backward");
         Adjoint* A = g->adj;
         const size_t st = (size_t)A->nf * A->field_elems;
         // the recompute buffers start as copies of X_0: their z ghost planes are constants

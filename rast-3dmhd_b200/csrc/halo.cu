@@ -90,6 +90,7 @@ void halo_free(r3d_gpu* g) {
 }
 
 void halo_reduce_limits(r3d_gpu* g) {
+    Range r("r3d.halo_reduce");
     Halo* h = g->halo;
     Nccl& n = nccl();
     nccl_ok(n.groupStart(), "ncclGroupStart");
@@ -99,6 +100,7 @@ void halo_reduce_limits(r3d_gpu* g) {
 }
 
 void halo_exchange(r3d_gpu* g) {
+    Range r("r3d.halo_exchange");
     Halo* h = g->halo;
     Nccl& n = nccl();
     const size_t plane = (size_t)g->geo.plane;

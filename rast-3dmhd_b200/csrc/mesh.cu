@@ -42,6 +42,7 @@ __global__ void mesh_reduce_kernel(r3dk::Scalars** s, int n) {
 }
 
 void exchange(r3d_mesh* m) {
+    Range r("r3d.mesh_exchange");
     for (size_t r = 0; r + 1 < m->slabs.size(); ++r) {
         r3d_gpu* a = m->slabs[r];
         r3d_gpu* b = m->slabs[r + 1];

@@ -163,12 +163,14 @@ void launch_dt_full_any(r3d_gpu* g) {
 
 // Queue one step (nstages substages) on the device.
 void enqueue_step_begin(r3d_gpu* g) {
+    Range r("r3d.step_begin");
     g->bnd.tpr = plume_tpr(g);
     if (g->halo) halo_reduce_limits(g);
     cuda_ok(r3dk::launch_step_begin(g->ph, g->dsc, g->stream), "step_begin");
 }
 
 void enqueue_stage(r3d_gpu* g, int s) {
+    Range r("r3d.stage");
     if (g->fp32) {
         r3dk::FieldSet32 fs = fieldset32(g);
         cuda_ok(r3dk::launch_stage_fp32(s, g->maps[g->cur], g->zmaps, g->geo, g->ph, g->lines, g->bg, fs, g->dsc,
@@ -186,6 +188,7 @@ void enqueue_stage(r3d_gpu* g, int s) {
 }
 
 void enqueue_step_end(r3d_gpu* g, int nstages) {
+    Range r("r3d.step_end");
     cuda_ok(r3dk::launch_step_end(g->dsc, g->stream), "step_end");
     if (nstages < 3) launch_dt_full_any(g);  // the next dt needs the limits of this partial-step state
 }
@@ -193,6 +196,7 @@ void enqueue_step_end(r3d_gpu* g, int nstages) {
 // Queue one step (nstages substages) on the device; with a Halo, the dt keys are reduced over
 // the slabs before the step and the ghost planes exchanged after every stage.
 void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_launches) {
+    Range step_range("r3d.step");
     g->bnd.tpr = plume_tpr(g);
     tm.begin();
     if (g->halo) halo_reduce_limits(g);
@@ -200,6 +204,7 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
     tm.end(2);
     ++launches;
     for (int s = 0; s < nstages; ++s) {
+        Range stage_range("r3d.stage");
         tm.begin();
         if (g->fp32) {
             r3dk::FieldSet32 fs = fieldset32(g);
@@ -604,6 +609,7 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
     return guarded([&] {
         if (!g || !st || !sc) throw std::invalid_argument("null argument");
         DeviceGuard dg(g->device);
+        Range r("r3d.upload");
         const Derived& d = g->d;
         const double* src[r3dk::kMaxFields] = {st->ru, st->rv, st->rw, st->ro, st->tt, st->bx, st->by, st->bz};
         for (int q = 0; q < g->nfields; ++q)
@@ -668,6 +674,7 @@ int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc) {
         if (!g || !st) throw std::invalid_argument("null argument");
         if (!g->uploaded) throw Error(R3D_ESTATE, "download before upload");
         DeviceGuard dg(g->device);
+        Range r("r3d.download");
         const Derived& d = g->d;
         double* dst[r3dk::kMaxFields] = {st->ru, st->rv, st->rw, st->ro, st->tt, st->bx, st->by, st->bz};
         if (g->fp32) {

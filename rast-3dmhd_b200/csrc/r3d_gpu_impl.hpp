@@ -4,6 +4,7 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <string>
@@ -77,6 +78,15 @@ struct DeviceGuard {
         cudaGetDevice(&now);
         if (prev >= 0 && now != prev) cudaSetDevice(prev);
     }
+};
+
+// NVTX range over a host scope ("r3d.step", "r3d.stage", ...), for profiler timelines; free
+// when no tool is attached.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
 };
 
 // CUDA-event spans of a queued step sequence (inactive when on == false).

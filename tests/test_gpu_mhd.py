@@ -69,3 +69,10 @@ def test_mhd_partial_step_bitexact(stages):
 def test_mhd_config2_grid_three_steps():
     """The MHD benchmark grid 126x126x256 (--beta 10 --rm 1, layer ampb 0.1 bfh 2 bzp 20, seed 7)."""
     check(["--npx", "126", "--npy", "126", "--npz", "256"] + MAG, 7, 3)
+
+
+@pytest.mark.gpu
+def test_mhd_config2_hundred_steps():
+    """The MHD benchmark case as stated: 126x126x256, --lmag 1 --beta 10 --rm 1, layer
+    ampb 0.1 bfh 2 bzp 20, seed 7, 100 RK3 steps, bit for bit (about 45 s of oracle time)."""
+    check(["--npx", "126", "--npy", "126", "--npz", "256"] + MAG, 7, 100)
