@@ -415,6 +415,7 @@ def main():
         clk.wait_first()
         barrier(pg)
         sc, tm = sim.run_timed(args.steps)       # synchronises on exit
+    refolds = sim.debug_dt_filter()              # full dt re-evaluations since the upload
     barrier(pg)
     total_ms = allmax(pg, tm["total_ms"])
     stage_avg_ms = tm["stage_ms"] / max(1, tm["stage_launches"])
@@ -485,7 +486,11 @@ def main():
                                           f"(NCCL ghost planes per stage, dt all-reduce per step)")},
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": int(tm["total_launches"]), "clocks": clk.summary(),
-               "final_dt": sc["dt"], "extra": extra}
+               "final_dt": sc["dt"],
+               "dt_refolds": {"count": refolds, "steps": args.warmup + args.steps,
+                              "note": "full re-evaluations of the third stage's filtered dt limits "
+                                      "(-1: slab handle, filter off)"},
+               "extra": extra}
         print(json.dumps(out))
     if pg is not None:
         pg.destroy_process_group()

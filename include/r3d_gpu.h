@@ -154,6 +154,16 @@ int r3d_gpu_fluxes(r3d_gpu* g, double* const* out);
  * usable.  0 (the default, restored by r3d_gpu_upload) switches it off. */
 int r3d_gpu_debug_tma_extra(r3d_gpu* g, unsigned int bytes);
 
+/* The third stage's time-step limits are folded through a filter: cells whose float estimates
+ * of the CFL limit and Mach term lie clearly beyond the previous step's limits widened by a
+ * relative margin (default 1/64) skip the exact FP64 evaluation, and when the folded result
+ * fails the check that makes this exact, the limits are evaluated again over the whole state
+ * (a "refold").  The dt is bit-identical either way.  Test hook: margin (NaN: unchanged) sets
+ * the margin - a negative one makes every full step refold - and *refolds (may be NULL)
+ * receives the number of refolds since the upload, or -1 on a slab handle, where the filter
+ * keeps only its exact running bounds. */
+int r3d_gpu_debug_dt_filter(r3d_gpu* g, double margin, int* refolds);
+
 /* Bytes of device memory held by g. */
 int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes);
 /* The CUDA stream (cudaStream_t) every kernel of g is launched on. */

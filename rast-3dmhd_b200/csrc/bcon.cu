@@ -113,8 +113,9 @@ cudaError_t launch_bcon(const Geometry& g, const Physics& ph, const Lines& L, co
 // partial step, to seed the reduction the next step starts from).
 // ---------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) dt_full_kernel(Geometry g, Physics ph, Lines L,
-                                                      FieldSet fs, Scalars* sc) {
+                                                      FieldSet fs, Scalars* sc, int only_refold) {
     __shared__ double red[5 * 8];
+    if (only_refold && *(volatile int*)&sc->refold == 0) return;  // uniform over the grid
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     double m1 = 1e300, m2 = 1e300, m3 = 1e300, m4 = 1e300, mu = 0.0;
@@ -139,10 +140,12 @@ __global__ void __launch_bounds__(256) dt_full_kernel(Geometry g, Physics ph, Li
 }
 
 cudaError_t launch_dt_full(const Geometry& g, const Physics& ph, const Lines& L,
-                           const FieldSet& fs, Scalars* sc, cudaStream_t st) {
+                           const FieldSet& fs, Scalars* sc, cudaStream_t st, int only_refold) {
     dim3 block(32, 8, 1);
-    dim3 grid((g.npx + 31) / 32, (g.npy + 7) / 8, (unsigned)min(g.npz, 64));
-    dt_full_kernel<<<grid, block, 0, st>>>(g, ph, L, fs, sc);
+    // the conditional form (after a filtered third stage) is a no-op in almost every step: a
+    // shallow grid keeps its cost to a few microseconds
+    dim3 grid((g.npx + 31) / 32, (g.npy + 7) / 8, (unsigned)min(g.npz, only_refold ? 2 : 64));
+    dt_full_kernel<<<grid, block, 0, st>>>(g, ph, L, fs, sc, only_refold);
     return cudaGetLastError();
 }
 
@@ -157,15 +160,34 @@ __global__ void step_begin_kernel(Physics ph, Scalars* sc) {
     m = (w2 < m) ? w2 : m;
     if (ph.lmag) m = (w3 < m) ? w3 : m;
     sc->dt = ph.sff * m;
-    sc->umach = sqrt(order_value(sc->umax));
+    const double u = order_value(sc->umax);
+    sc->umach = sqrt(u);
+    // thresholds of this step's filtered fold: the previous limits widened by the margin (a
+    // margin < 0 forces the re-evaluation path; thr_on == 0 leaves only the exact running bounds)
+    sc->thr_w1 = sc->thr_on ? w0 * (1.0 + sc->thr_margin) : 1e308;
+    sc->thr_um = sc->thr_on ? u * (1.0 - sc->thr_margin) : 0.0;
     sc->wmin[0] = sc->wmin[1] = sc->wmin[2] = sc->wmin[3] = order_key(1e300);
     sc->umax = order_key(0.0);
 }
 
-__global__ void step_end_kernel(Scalars* sc) {
+// check != 0 (after a full step on a handle with the threshold filter): the skipped cells have
+// ww1 > thr_w1 and a Mach term < thr_um, so the folded limits are exact iff the minimum found
+// is <= thr_w1 and the maximum >= thr_um; otherwise clear them and request the full evaluation
+// (dt_full_kernel with only_refold).
+__global__ void step_end_kernel(Scalars* sc, int check) {
     sc->nit += 1;
     sc->timc += sc->dt;
     sc->timt = sc->timi + sc->timc;
+    int refold = 0;
+    if (check && sc->thr_on) {
+        refold = !(order_value(sc->wmin[0]) <= sc->thr_w1) || !(order_value(sc->umax) >= sc->thr_um);
+        if (refold) {
+            sc->refolds += 1;
+            sc->wmin[0] = sc->wmin[1] = sc->wmin[2] = sc->wmin[3] = order_key(1e300);
+            sc->umax = order_key(0.0);
+        }
+    }
+    sc->refold = refold;
 }
 
 __global__ void reset_reduction_kernel(Scalars* sc) {
@@ -177,8 +199,8 @@ cudaError_t launch_step_begin(const Physics& ph, Scalars* sc, cudaStream_t st) {
     step_begin_kernel<<<1, 1, 0, st>>>(ph, sc);
     return cudaGetLastError();
 }
-cudaError_t launch_step_end(Scalars* sc, cudaStream_t st) {
-    step_end_kernel<<<1, 1, 0, st>>>(sc);
+cudaError_t launch_step_end(Scalars* sc, cudaStream_t st, int check) {
+    step_end_kernel<<<1, 1, 0, st>>>(sc, check);
     return cudaGetLastError();
 }
 cudaError_t launch_reset_reduction(Scalars* sc, cudaStream_t st) {

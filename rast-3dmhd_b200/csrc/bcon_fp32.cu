@@ -74,8 +74,10 @@ __global__ void __launch_bounds__(256) bcon_fp32_kernel(Geometry g, Physics ph, 
 }
 
 __global__ void __launch_bounds__(256) dt_full_fp32_kernel(Geometry g, Physics ph, Lines L,
-                                                           Background bg, FieldSet32 fs, Scalars* sc) {
+                                                           Background bg, FieldSet32 fs, Scalars* sc,
+                                                           int only_refold) {
     __shared__ double red[5 * 8];
+    if (only_refold && *(volatile int*)&sc->refold == 0) return;  // uniform over the grid
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     double m1 = 1e300, m2 = 1e300, m3 = 1e300, m4 = 1e300, mu = 0.0;
@@ -128,9 +130,10 @@ cudaError_t launch_bcon_fp32(const Geometry& g, const Physics& ph, const Lines& 
 }
 
 cudaError_t launch_dt_full_fp32(const Geometry& g, const Physics& ph, const Lines& L,
-                                const Background& bg, const FieldSet32& fs, Scalars* sc, cudaStream_t st) {
-    dim3 block(32, 8, 1), grid((g.npx + 31) / 32, (g.npy + 7) / 8, (unsigned)min(g.npz, 64));
-    dt_full_fp32_kernel<<<grid, block, 0, st>>>(g, ph, L, bg, fs, sc);
+                                const Background& bg, const FieldSet32& fs, Scalars* sc, cudaStream_t st,
+                                int only_refold) {
+    dim3 block(32, 8, 1), grid((g.npx + 31) / 32, (g.npy + 7) / 8, (unsigned)min(g.npz, only_refold ? 2 : 64));
+    dt_full_fp32_kernel<<<grid, block, 0, st>>>(g, ph, L, bg, fs, sc, only_refold);
     return cudaGetLastError();
 }
 

@@ -36,6 +36,7 @@ struct Physics {
     double gam[3], zeta[3];
     int lrot, lmag;
     int kappa_const;  // rkapa == 1 and dkapa == 0 on every plane (exact shortcut)
+    float gamma_f, ogamma_f, obeta_f;  // float copies for the estimates of the dt filter
 };
 
 // 1D metric tables (device pointers).
@@ -69,6 +70,16 @@ struct Scalars {
     unsigned long long wmin[4];  // keys of min(ww1), min(ww2), min(ww3), min(vv)
     unsigned long long umax;     // key of max(ogamma*uu/tt)
     double mass, energy;         // diagnostics (r3d_gpu_totals)
+    // Threshold filter of the third stage's limits (fold_dt_filtered): on whole-domain handles,
+    // cells whose estimated ww1 exceeds thr_w1 and whose Mach term is below thr_um skip the exact
+    // evaluation.  step_begin sets the thresholds from the previous limits widened by
+    // thr_margin; step_end sets refold when the filtered minimum/maximum fails the check, and
+    // the limits are then evaluated again over the whole state.
+    int thr_on;
+    int refold;
+    int refolds;  // number of re-evaluations since the upload (diagnostic)
+    double thr_margin;
+    double thr_w1, thr_um;
 };
 
 // Total order on doubles as unsigned keys: key(a) < key(b) iff a < b (NaN excluded).

@@ -154,11 +154,14 @@ double plume_tpr(const r3d_gpu* g) {
     return (g->p.tc != 0.0) ? g->p.tp + (1.0 - g->p.tp) * std::exp(-timt / g->p.tc) : g->p.tp;
 }
 
-void launch_dt_full_any(r3d_gpu* g) {
+void launch_dt_full_any(r3d_gpu* g, int only_refold) {
     if (g->fp32)
-        cuda_ok(r3dk::launch_dt_full_fp32(g->geo, g->ph, g->lines, g->bg, fieldset32(g), g->dsc, g->stream), "dt_full32");
+        cuda_ok(r3dk::launch_dt_full_fp32(g->geo, g->ph, g->lines, g->bg, fieldset32(g), g->dsc, g->stream,
+                                          only_refold),
+                "dt_full32");
     else
-        cuda_ok(r3dk::launch_dt_full(g->geo, g->ph, g->lines, fieldset(g), g->dsc, g->stream), "dt_full");
+        cuda_ok(r3dk::launch_dt_full(g->geo, g->ph, g->lines, fieldset(g), g->dsc, g->stream, only_refold),
+                "dt_full");
 }
 
 // Queue one step (nstages substages) on the device.
@@ -189,8 +192,9 @@ void enqueue_stage(r3d_gpu* g, int s) {
 
 void enqueue_step_end(r3d_gpu* g, int nstages) {
     Range r("r3d.step_end");
-    cuda_ok(r3dk::launch_step_end(g->dsc, g->stream), "step_end");
+    cuda_ok(r3dk::launch_step_end(g->dsc, g->stream, nstages == 3 ? 1 : 0), "step_end");
     if (nstages < 3) launch_dt_full_any(g);  // the next dt needs the limits of this partial-step state
+    else if (g->dt_filter) launch_dt_full_any(g, 1);  // only if the filtered limits failed the check
 }
 
 // Queue one step (nstages substages) on the device; with a Halo, the dt keys are reduced over
@@ -230,10 +234,13 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
         }
     }
     tm.begin();
-    cuda_ok(r3dk::launch_step_end(g->dsc, g->stream), "step_end");
+    cuda_ok(r3dk::launch_step_end(g->dsc, g->stream, nstages == 3 ? 1 : 0), "step_end");
     ++launches;
     if (nstages < 3) {  // the next dt needs the limits of this (partial-step) state
         launch_dt_full_any(g);
+        ++launches;
+    } else if (g->dt_filter) {  // re-evaluation, only if the filtered limits failed the check
+        launch_dt_full_any(g, 1);
         ++launches;
     }
     tm.end(2);
@@ -468,6 +475,7 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             g->geo.npz = nloc;
             g->geo.top_edge = z0 == 0 ? 1 : 0;
             g->geo.bot_edge = z0 + nloc == p->npz ? 1 : 0;
+            g->dt_filter = z0 == 0 && nloc == p->npz;
             g->geo.pitch = (d.nx + 15) / 16 * 16;
             g->geo.plane = g->geo.pitch * d.ny;
             if (g->geo.plane * d.nz >= (int64_t(1) << 31))
@@ -533,6 +541,7 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             for (int s = 0; s < 3; ++s) { ph.gam[s] = d.gam[s]; ph.zeta[s] = d.zeta[s]; }
             ph.lrot = p->lrot; ph.lmag = p->lmag;
             ph.kappa_const = 1;
+            ph.gamma_f = (float)ph.gamma; ph.ogamma_f = (float)ph.ogamma; ph.obeta_f = (float)ph.obeta;
             r3dk::Boundary& b = g->bnd;
             if (p->tp != 0.0 && (p->itcon == 0 || p->itcon == 1)) b.top_mode = p->itcon == 0 ? 2 : 3;
             else if (p->itcon == 4) b.top_mode = 4;
@@ -657,6 +666,8 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
         r3dk::Scalars h{};
         h.dt = sc->dt; h.timc = sc->timc; h.timt = sc->timt; h.timi = sc->timi;
         h.umach = sc->umach; h.tb = sc->tb; h.nit = sc->nit;
+        h.thr_on = g->dt_filter ? 1 : 0;
+        h.thr_margin = g->thr_margin;
         *g->hsc = h;
         cuda_ok(cudaMemcpyAsync(g->dsc, g->hsc, sizeof(h), cudaMemcpyHostToDevice, g->stream), "upload scalars");
         g->bnd.tb = sc->tb;
@@ -756,6 +767,26 @@ int r3d_gpu_debug_tma_extra(r3d_gpu* g, unsigned int bytes) {
         cuda_ok(cudaMemcpyAsync(&g->dsc->tx_extra, &bytes, sizeof bytes, cudaMemcpyHostToDevice, g->stream),
                 "tx_extra");
         cuda_ok(cudaStreamSynchronize(g->stream), "tx_extra");
+    });
+}
+
+int r3d_gpu_debug_dt_filter(r3d_gpu* g, double margin, int* refolds) {
+    return guarded([&] {
+        if (!g) throw std::invalid_argument("null handle");
+        DeviceGuard dg(g->device);
+        if (!std::isnan(margin)) {
+            g->thr_margin = margin;
+            cuda_ok(cudaMemcpyAsync(&g->dsc->thr_margin, &g->thr_margin, sizeof(double), cudaMemcpyHostToDevice,
+                                    g->stream),
+                    "thr_margin");
+        }
+        if (refolds) {
+            cuda_ok(cudaMemcpyAsync(&g->hsc->refolds, &g->dsc->refolds, sizeof(int), cudaMemcpyDeviceToHost,
+                                    g->stream),
+                    "refolds");
+        }
+        cuda_ok(cudaStreamSynchronize(g->stream), "dt filter");
+        if (refolds) *refolds = g->dt_filter ? g->hsc->refolds : -1;
     });
 }
 

@@ -57,6 +57,10 @@ struct r3d_gpu {
     bool own_stream = true;
     r3dg::Halo* halo = nullptr;              // ghost-plane exchange with other slabs (NCCL)
     double* fscr = nullptr;                  // r3d_gpu_fluxes scratch: X', Z', F (nfields each)
+    // threshold filter of the third stage's limits (whole-domain handles only: a slab's own
+    // limits are not the domain's, and its thresholds would come from the reduced ones)
+    bool dt_filter = false;
+    double thr_margin = 1.0 / 64.0;
 };
 
 namespace r3dg {
@@ -119,7 +123,7 @@ struct Timer {
 CUtensorMap field_map(void* base, int64_t nx, int64_t ny, int64_t nz, int64_t pitch, int64_t plane,
                       cuuint32_t box_x, cuuint32_t box_y, CUtensorMapDataType type, size_t esize);
 r3dk::FieldSet fieldset(const r3d_gpu* g);
-void launch_dt_full_any(r3d_gpu* g);
+void launch_dt_full_any(r3d_gpu* g, int only_refold = 0);
 void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_launches);
 void pull_scalars(r3d_gpu* g, r3d_scalars* sc);
 

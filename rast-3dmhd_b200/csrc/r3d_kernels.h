@@ -54,7 +54,8 @@ cudaError_t launch_bcon_fp32(const Geometry& g, const Physics& ph, const Lines& 
                              const Background& bg, const FieldSet32& fs, Scalars* sc, int with_dt,
                              cudaStream_t st);
 cudaError_t launch_dt_full_fp32(const Geometry& g, const Physics& ph, const Lines& L,
-                                const Background& bg, const FieldSet32& fs, Scalars* sc, cudaStream_t st);
+                                const Background& bg, const FieldSet32& fs, Scalars* sc, cudaStream_t st,
+                                int only_refold = 0);
 cudaError_t launch_totals_fp32(const Geometry& g, const Physics& ph, const Background& bg,
                                const FieldSet32& fs, Scalars* sc, cudaStream_t st);
 
@@ -66,10 +67,12 @@ cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& 
                               int kchunk, cudaStream_t st, bool emit_rhs = false);
 cudaError_t launch_bcon(const Geometry& g, const Physics& ph, const Lines& L, const Boundary& b,
                         const FieldSet& fs, Scalars* sc, int with_dt, cudaStream_t st);
+// only_refold: run only if step_end requested a re-evaluation (Scalars::refold)
 cudaError_t launch_dt_full(const Geometry& g, const Physics& ph, const Lines& L,
-                           const FieldSet& fs, Scalars* sc, cudaStream_t st);
+                           const FieldSet& fs, Scalars* sc, cudaStream_t st, int only_refold = 0);
 cudaError_t launch_step_begin(const Physics& ph, Scalars* sc, cudaStream_t st);
-cudaError_t launch_step_end(Scalars* sc, cudaStream_t st);
+// check: verify the filtered limits of a full step (Scalars::thr_*), request a refold if needed
+cudaError_t launch_step_end(Scalars* sc, cudaStream_t st, int check = 0);
 cudaError_t launch_reset_reduction(Scalars* sc, cudaStream_t st);
 cudaError_t launch_totals(const Geometry& g, const Physics& ph, const FieldSet& fs, Scalars* sc,
                           cudaStream_t st);

@@ -36,34 +36,58 @@ __device__ __forceinline__ void dt_terms(const Physics& ph, double ru, double rv
 __device__ __forceinline__ double fold_min(double acc, double v);
 __device__ __forceinline__ double fold_max(double acc, double v);
 
-// Fold one cell's time-step limits into running minima m1..m4 and maximum mu, evaluating the
-// costly FP64 ww1 = dd/sqrt(c^2) and Mach term (a reciprocal, two divisions, two square roots)
-// only for cells that can change m1 or mu.  FP32 estimates of both, with relative error below
-// 2^-18 (about twenty float operations on positive quantities, each correctly rounded or within
-// 2 ulp), are compared with the running values under a 2^-12 margin: a cell whose estimate is
-// clearly worse cannot be the minimum (maximum) and is skipped; every other cell - including any
-// cell whose estimate is not finite, and every cell while the running maximum is below 1e-30,
-// where float underflow voids the bound - takes the FP64 path.  The running values therefore
-// equal those of folding the FP64 values of every cell.
-__device__ __forceinline__ void fold_dt_terms_filtered(const Physics& ph, double ru, double rv,
-                                                       double rw, double ro, double tt, double dd,
-                                                       double rkap, double& m1, double& m2,
-                                                       double& m3, double& mu) {
-    m2 = fold_min(m2, 0.5 * dd * dd * ph.repr * ph.cv * ro / rkap);  // src/step.cpp:192-193
-    m3 = fold_min(m3, 0.375 * dd * dd * ph.re * ro);                 // src/step.cpp:194
+// True when x is positive and 2^-30 <= x < 2^31 (one integer compare on the high word): the
+// window in which the float estimates below keep their error bound.
+__device__ __forceinline__ bool est_window(double x) {
+    return (unsigned)__double2hiint(x) - 0x3e100000u < 0x03d00000u;
+}
+
+// Fold one cell's time-step limits into running minima m1..m4 and maximum mu.  The cheap limits
+// (ww2, ww3, vv: products of the cell's spacing and density) are folded exactly.  The costly
+// FP64 ww1 = dd/sqrt(c^2) and Mach term (a reciprocal, two divisions, two square roots) are
+// evaluated only for cells that can change m1 or mu: float estimates of both, with relative
+// error below 2^-17 (at most thirty float operations on positive quantities, each correctly
+// rounded or within 2 ulp, inputs in the est_window range), are compared under a 2^-12 margin
+// with b1 = min(m1, t1) and bu = max(mu, tu).  A cell is skipped only when its estimates are
+// clearly worse than both bounds; cells outside the window, with a non-finite estimate, or
+// while bu <= 2^-40 (where float underflow voids the bound on the Mach term) are evaluated.
+// With t1 = +huge and tu = 0 the running values equal those of folding the FP64 values of every
+// cell.  With thresholds t1, tu the skipped cells have ww1 > t1 and Mach term < tu, so the
+// folded limits over the whole domain are exact whenever the final minimum is <= t1 and the
+// final maximum is >= tu (checked by step_end_kernel, which requests a full re-evaluation
+// otherwise).  Expressions and operation order of the exact path are those of dt_terms.
+template <bool KC, bool MHD>
+__device__ __forceinline__ void fold_dt_filtered(const Physics& ph, double ru, double rv,
+                                                 double rw, double ro, double tt, double b2sum,
+                                                 double dd, double rkap, double t1, double tu,
+                                                 double& m1, double& m2, double& m3, double& m4,
+                                                 double& mu) {
+    m2 = fold_min(m2, KC ? 0.5 * dd * dd * ph.repr * ph.cv * ro                  // src/step.cpp:192-193
+                         : 0.5 * dd * dd * ph.repr * ph.cv * ro / rkap);
+    m3 = fold_min(m3, 0.375 * dd * dd * ph.re * ro);                            // src/step.cpp:194
+    if constexpr (MHD) m4 = fold_min(m4, 0.5 * dd * dd * ph.rm);
     const float rof = (float)ro, ttf = (float)tt;
     const float ruf = (float)ru, rvf = (float)rv, rwf = (float)rw;
     const float rf = __fdividef(1.0f, rof);
     const float uuf = (ruf * ruf + rvf * rvf + rwf * rwf) * rf * rf;
-    const float umf = __fdividef((float)ph.ogamma * uuf, ttf);
-    const float gtf = (float)ph.gamma * ttf;
-    const float c2f = uuf + gtf + 2.0f * sqrtf(uuf * gtf);
+    const float umf = __fdividef(ph.ogamma_f * uuf, ttf);
+    const float gtf = ph.gamma_f * ttf;
+    float c2f;
+    if constexpr (MHD) {
+        const float b2f = (float)b2sum * ph.obeta_f * rf;
+        c2f = uuf + gtf + b2f + 2.0f * sqrtf(uuf * (gtf + b2f));
+    } else {
+        c2f = uuf + gtf + 2.0f * sqrtf(uuf * gtf);
+    }
     const float w1f = __fdividef((float)dd, sqrtf(c2f));
-    const bool skip_um = (double)umf * (1.0 + 1.0 / 4096.0) < mu && mu > 1e-30;
-    const bool skip_w1 = (double)w1f * (1.0 - 1.0 / 4096.0) > m1;
+    const double b1 = (t1 < m1) ? t1 : m1;
+    const double bu = (mu < tu) ? tu : mu;
+    const bool ok = est_window(ro) && est_window(tt) && est_window(dd);
+    const bool skip_um = ok && bu > 0x1p-40 && (double)umf * (1.0 + 1.0 / 4096.0) < bu;
+    const bool skip_w1 = ok && (double)w1f * (1.0 - 1.0 / 4096.0) > b1;
     if (skip_um && skip_w1) return;
     double w1, w2, w3, w4, um;
-    dt_terms<false>(ph, ru, rv, rw, ro, tt, 0.0, dd, rkap, w1, w2, w3, w4, um);
+    dt_terms<KC>(ph, ru, rv, rw, ro, tt, MHD ? b2sum : 0.0, dd, rkap, w1, w2, w3, w4, um);
     m1 = fold_min(m1, w1);
     mu = fold_max(mu, um);
 }

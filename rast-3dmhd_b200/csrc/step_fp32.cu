@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(NT, 3)
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kRawBytes + kDerBytes + kZBytes);
     uint64_t* zbars = bars + NRAW;
     __shared__ int s_abort;
+    __shared__ double s_thr[2];  // third stage: thresholds of the dt filter (thr_w1, thr_um)
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
@@ -137,6 +138,10 @@ __global__ void __launch_bounds__(NT, 3)
     if (tid == 0) {
         s_abort = (*(volatile int*)&sc->err != kErrNone) ? 2 : 0;
         tx_extra = sc->tx_extra;
+        if (STAGE == 2) {
+            s_thr[0] = sc->thr_w1;
+            s_thr[1] = sc->thr_um;
+        }
         for (int b = 0; b < NRAW + NZS; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
     }
@@ -323,8 +328,9 @@ __global__ void __launch_bounds__(NT, 3)
         }
         if (STAGE == 2 && !edge) {  // dt limits, FP64 values on full state (filtered)
             const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[k]);
-            fold_dt_terms_filtered(ph, xn[0], xn[1], xn[2], bg.r[k] + (double)xn[3],
-                                   bg.t[k] + (double)xn[4], dd, L.rkapa[k], m1, m2, m3, mu);
+            fold_dt_filtered<false, false>(ph, xn[0], xn[1], xn[2], bg.r[k] + (double)xn[3],
+                                           bg.t[k] + (double)xn[4], 0.0, dd, L.rkapa[k], s_thr[0],
+                                           s_thr[1], m1, m2, m3, m4, mu);
         }
 #undef RW_
 #undef DV_

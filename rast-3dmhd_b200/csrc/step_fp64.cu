@@ -80,6 +80,8 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
     double* der = reinterpret_cast<double*>(smem + S::raw_bytes);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::raw_bytes + S::der_bytes);
     __shared__ int s_abort;
+    __shared__ int s_filter;     // third stage: threshold-filtered dt fold (Scalars::thr_on)
+    __shared__ double s_thr[2];  // its thresholds thr_w1, thr_um
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
@@ -123,6 +125,11 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
         // a CTA that finds an earlier timeout recorded leaves before issuing any copy
         s_abort = (*(volatile int*)&sc->err != kErrNone) ? 2 : 0;
         tx_extra = sc->tx_extra;
+        if (STAGE == 2) {
+            s_filter = sc->thr_on;
+            s_thr[0] = sc->thr_w1;
+            s_thr[1] = sc->thr_um;
+        }
         for (int b = 0; b < NRAW; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
     }
@@ -457,14 +464,19 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[k]);
                 double b2sum = 0.0;
                 if constexpr (MHD) b2sum = xn[5] * xn[5] + xn[6] * xn[6] + xn[7] * xn[7];
-                double w1, w2, w3, w4, um;
-                dt_terms<KC>(ph, xn[0], xn[1], xn[2], xn[3], xn[4], b2sum, dd, L.rkapa[k], w1, w2,
-                             w3, w4, um);
-                m1 = fold_min(m1, w1);
-                m2 = fold_min(m2, w2);
-                m3 = fold_min(m3, w3);
-                m4 = fold_min(m4, w4);
-                mu = fold_max(mu, um);
+                if (s_filter) {
+                    fold_dt_filtered<KC, MHD>(ph, xn[0], xn[1], xn[2], xn[3], xn[4], b2sum, dd,
+                                              L.rkapa[k], s_thr[0], s_thr[1], m1, m2, m3, m4, mu);
+                } else {
+                    double w1, w2, w3, w4, um;
+                    dt_terms<KC>(ph, xn[0], xn[1], xn[2], xn[3], xn[4], b2sum, dd, L.rkapa[k], w1,
+                                 w2, w3, w4, um);
+                    m1 = fold_min(m1, w1);
+                    m2 = fold_min(m2, w2);
+                    m3 = fold_min(m3, w3);
+                    m4 = fold_min(m4, w4);
+                    mu = fold_max(mu, um);
+                }
             }
 #undef RW_
 #undef DV_

@@ -109,6 +109,7 @@ def lib():
         L.r3d_gpu_run_timed.argtypes = [vp, ip, ctypes.POINTER(Scalars), ctypes.POINTER(Timing)]
         L.r3d_gpu_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.r3d_gpu_debug_tma_extra.argtypes = [vp, ctypes.c_uint]
+        L.r3d_gpu_debug_dt_filter.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         L.r3d_gpu_fluxes.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
         L.r3d_setup_host_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(_HostStateC),
                                           ctypes.POINTER(Scalars)]
@@ -334,6 +335,14 @@ class GpuSim:
     def debug_tma_extra(self, nbytes: int):
         """Test hook: make the stage kernels' bounded TMA waits run out (0 switches it off)."""
         _check(lib().r3d_gpu_debug_tma_extra(self.h, nbytes))
+
+    def debug_dt_filter(self, margin: float = float("nan")) -> int:
+        """Test hook of the third stage's dt filter: set its relative margin (NaN: unchanged; < 0
+        forces a full re-evaluation every step) and return the re-evaluations since the upload
+        (-1 on a slab handle)."""
+        n = ctypes.c_int(0)
+        _check(lib().r3d_gpu_debug_dt_filter(self.h, margin, ctypes.byref(n)))
+        return n.value
 
     # ---- discrete adjoint (FP64) ----
     def _fields(self):
