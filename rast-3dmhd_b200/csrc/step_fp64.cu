@@ -172,19 +172,21 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
 
     for (int k = kb; k <= ke; ++k) {
         const int q = k - (kb - 1);
-        if (!derive(k + 1)) s_abort = 1;
-        __syncthreads();
-        if (s_abort) break;
-        if (tid == 0 && k + 2 <= ke + 1) {
-            fence_proxy_async();
-            issue(k + 2);
-        }
+        // the next plane's accumulators: issued before the derive phase and the barrier, so
+        // their latency hides behind a whole plane of work
         double zq[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) zq[f] = zn[f];
         if (STAGE > 0 && active && k < ke) {
 #pragma unroll
             for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][(k + 1) * PL + col];
+        }
+        if (!derive(k + 1)) s_abort = 1;
+        __syncthreads();
+        if (s_abort) break;
+        if (tid == 0 && k + 2 <= ke + 1) {
+            fence_proxy_async();
+            issue(k + 2);
         }
         if (active) {
             const int nc = k * PL + col;
