@@ -61,6 +61,10 @@ struct r3d_gpu {
     // limits are not the domain's, and its thresholds would come from the reduced ones)
     bool dt_filter = false;
     double thr_margin = 1.0 / 64.0;
+    // two whole steps captured as a CUDA graph, one per state-buffer parity at capture (r3d_gpu_run
+    // replays it; six stages leave the parity unchanged)
+    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+    int64_t steps_enqueued = 0;
 };
 
 namespace r3dg {
