@@ -719,8 +719,14 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
             }
         } else {
             for (int q = 0; q < g->nfields; ++q) {
-                cuda_ok(cudaMemcpy2DAsync(g->X[0][q], g->geo.pitch * sizeof(double), src[q], d.nx * sizeof(double),
-                                          d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyHostToDevice, g->stream),
+                // one contiguous host-to-device copy into the accumulator (dead between steps:
+                // the first stage rewrites it), then the re-pitch on the device - a pitched
+                // host-to-device copy runs at about half the link rate
+                const size_t n = (size_t)d.nx * d.ny * d.nz;
+                cuda_ok(cudaMemcpyAsync(g->Z[q], src[q], n * sizeof(double), cudaMemcpyHostToDevice, g->stream),
+                        "upload state");
+                cuda_ok(cudaMemcpy2DAsync(g->X[0][q], g->geo.pitch * sizeof(double), g->Z[q], d.nx * sizeof(double),
+                                          d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyDeviceToDevice, g->stream),
                         "upload state");
                 // the second buffer gets the same contents on the device (its z ghost planes are
                 // never written by a stage)
