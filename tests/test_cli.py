@@ -6,50 +6,15 @@ reference's binary layout (src/main.cpp:42-93).  CPU tests cover argument handli
 test runs a short job and compares the dumped state with the oracle bit for bit.
 """
 import os
-import struct
 import subprocess
 
 import numpy as np
 import pytest
 
 from conftest import ROOT as REPO
+from r3d_b200 import gstate
 
 BIN = os.path.join(REPO, "rast-3dmhd_b200", "bin", "r3d_b200")
-FIELDS27 = ["ru", "rv", "rw", "ro", "tt", "uu", "vv", "ww", "fu", "fv", "fw", "fr", "ft", "zru", "zrv",
-            "zrw", "zro", "ztt", "ww1", "ww2", "ww3", "bx", "by", "bz", "zbx", "zby", "zbz"]
-LINES14 = ["exx", "dxxdx", "d2xxdx2", "ddx", "wyy", "dyydy", "d2yydy2", "ddy", "zee", "dzzdz",
-           "d2zzdz2", "ddz", "rkapa", "dkapa"]
-
-
-def read_gstate(path):
-    """Reader of the gstate layout: magic, nf, n1, 13 ints, 27 doubles, nf counted 3D arrays,
-    n1 counted 1D arrays, int64 -1."""
-    with open(path, "rb") as f:
-        b = f.read()
-    magic, nf, n1 = struct.unpack_from("<iii", b, 0)
-    assert magic == 1129928788 and nf == 27 and n1 == 14
-    hdr = struct.unpack_from("<13i", b, 12)
-    sc = struct.unpack_from("<27d", b, 12 + 52)
-    off = 12 + 52 + 216
-    nx, ny, nz = hdr[:3]
-    arrays = {}
-    for name in FIELDS27:
-        (cnt,) = struct.unpack_from("<q", b, off)
-        off += 8
-        assert cnt == nx * ny * nz
-        arrays[name] = np.frombuffer(b, dtype="<f8", count=cnt, offset=off).reshape(nz, ny, nx)
-        off += 8 * cnt
-    lines = {}
-    for name in LINES14:
-        (cnt,) = struct.unpack_from("<q", b, off)
-        off += 8
-        lines[name] = np.frombuffer(b, dtype="<f8", count=cnt, offset=off)
-        off += 8 * cnt
-    (end,) = struct.unpack_from("<q", b, off)
-    assert end == -1 and off + 8 == len(b)
-    return hdr, sc, arrays, lines
-
-
 def run(args, cwd, timeout=300):
     return subprocess.run([BIN] + args, cwd=cwd, capture_output=True, text=True, timeout=timeout)
 
@@ -90,19 +55,40 @@ def test_cli_run_dumps_match_oracle(tmp_path):
     assert names == ["gstate.start.000.0000", "gstate.step.000.0002", "gstate.step.000.0004",
                      "gstate.step.000.0005"]
     o = Oracle(flags).init(62659)
-    hdr, sc, arr, lines = read_gstate(os.path.join(tmp_path, "gstate.start.000.0000"))
-    assert hdr[:3] == (22, 14, 26) and hdr[6] == 0
+    g0 = gstate.read(os.path.join(tmp_path, "gstate.start.000.0000"))
+    assert (g0.header["nx"], g0.header["ny"], g0.header["nz"]) == (22, 14, 26) and g0.header["nit"] == 0
     for n in ("ru", "rv", "rw", "ro", "tt"):
-        assert np.array_equal(interior(arr[n]), interior(o.field(n))), n
-    for n in LINES14:
-        assert np.array_equal(lines[n], o.line(n)), n
+        assert np.array_equal(interior(g0.fields[n]), interior(o.field(n))), n
+    for n in gstate.LINES:
+        assert np.array_equal(g0.lines[n], o.line(n)), n
     for s in range(5):
         o.step()
-    hdr, sc, arr, _ = read_gstate(os.path.join(tmp_path, "gstate.step.000.0005"))
+    g5 = gstate.read(os.path.join(tmp_path, "gstate.step.000.0005"))
     osc = o.scalars()
-    assert hdr[6] == 5 and sc[0] == osc["dt"] and sc[1] == osc["timc"]
+    assert g5.header["nit"] == 5 and g5.scalars["dt"] == osc["dt"] and g5.scalars["timc"] == osc["timc"]
     for n in ("ru", "rv", "rw", "ro", "tt"):
-        assert np.array_equal(interior(arr[n]), interior(o.field(n))), n
+        assert np.array_equal(interior(g5.fields[n]), interior(o.field(n))), n
     # --dump-mode 0: progress lines only
     r = run(flags + ["--dump-mode", "0"], tmp_path / "..")
     assert r.returncode == 0 and sum(ln.startswith("NIT ") for ln in r.stderr.splitlines()) == 3
+
+
+def test_gstate_reader_rejects_damaged_files(tmp_path):
+    """The reader checks magic, counts, array lengths and the end marker."""
+    import struct
+    nx, ny, nz = 3, 2, 2
+    parts = [struct.pack("<iii", gstate.MAGIC, 27, 14), struct.pack("<13i", nx, ny, nz, *([0] * 10)),
+             struct.pack("<27d", *([0.5] * 27))]
+    for _ in range(27):
+        parts += [struct.pack("<q", nx * ny * nz), np.arange(nx * ny * nz, dtype="<f8").tobytes()]
+    for _ in range(14):
+        parts += [struct.pack("<q", 4), np.ones(4, dtype="<f8").tobytes()]
+    good = b"".join(parts + [struct.pack("<q", -1)])
+    (tmp_path / "ok").write_bytes(good)
+    g = gstate.read(str(tmp_path / "ok"))
+    assert g.fields["ro"].shape == (nz, ny, nx) and g.fields["tt"][1, 1, 2] == 11.0
+    assert g.scalars["dt"] == 0.5 and list(g.lines) == gstate.LINES
+    for bad in (good[:-8], b"\0" * 4 + good[4:], good[:200]):
+        (tmp_path / "bad").write_bytes(bad)
+        with pytest.raises(ValueError):
+            gstate.read(str(tmp_path / "bad"))
