@@ -97,6 +97,26 @@ __global__ void totals_kernel(r3dk::Geometry g, r3dk::Physics ph, FieldSet fs, r
     }
 }
 
+// FP32-bulk state <-> the reference layout in FP64: dev32 (pitched) = (float)(host - bg[k]) on
+// upload, host = bg[k] + (double)dev32 on download, for one field of nx*ny*nz cells.  bg is the
+// static background column (rho or T), or null for the momenta.
+__global__ void to_fp32_kernel(float* out, int64_t pitch, int64_t plane, const double* in, int64_t nx,
+                               int64_t ny, int64_t nz, const double* bg) {
+    const int64_t n = nx * ny * nz;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+        out[k * plane + j * pitch + i] = (float)(in[c] - (bg ? bg[k] : 0.0));
+    }
+}
+__global__ void from_fp32_kernel(double* out, const float* in, int64_t pitch, int64_t plane, int64_t nx,
+                                 int64_t ny, int64_t nz, const double* bg) {
+    const int64_t n = nx * ny * nz;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+        out[c] = (bg ? bg[k] : 0.0) + (double)in[k * plane + j * pitch + i];
+    }
+}
+
 }  // namespace
 
 namespace r3dk {
@@ -148,6 +168,37 @@ void background_columns(const r3d_gpu* g, std::vector<double>& R, std::vector<do
         T[k] = t[src];
     }
 }
+
+// A temporary FP64 field in the reference layout plus the rho / T background columns on the
+// device, for the FP32-bulk upload and download (freed when it goes out of scope, after the
+// stream has drained).
+struct Fp64Staging {
+    r3d_gpu* g;
+    size_t n = 0;
+    double* buf = nullptr;
+    double* cols = nullptr;  // R[nz], T[nz]
+    explicit Fp64Staging(r3d_gpu* gg) : g(gg) {
+        const Derived& d = g->d;
+        n = (size_t)d.nx * d.ny * d.nz;
+        std::vector<double> R, T;
+        background_columns(g, R, T);
+        cuda_ok(cudaMalloc(&buf, n * sizeof(double)), "cudaMalloc(staging)");
+        cuda_ok(cudaMalloc(&cols, 2 * R.size() * sizeof(double)), "cudaMalloc(staging)");
+        R.insert(R.end(), T.begin(), T.end());
+        cuda_ok(cudaMemcpyAsync(cols, R.data(), R.size() * sizeof(double), cudaMemcpyHostToDevice, g->stream),
+                "staging columns");
+        cuda_ok(cudaStreamSynchronize(g->stream), "staging columns");  // R is a host temporary
+    }
+    ~Fp64Staging() {
+        cudaStreamSynchronize(g->stream);
+        cudaFree(buf);
+        cudaFree(cols);
+    }
+    Fp64Staging(const Fp64Staging&) = delete;
+    Fp64Staging& operator=(const Fp64Staging&) = delete;
+    const double* bg(int q) const { return q == 3 ? cols : (q == 4 ? cols + g->d.nz : nullptr); }
+    unsigned blocks() const { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
+};
 
 double plume_tpr(const r3d_gpu* g) {
     const double timt = g->host_timc + g->host_timi;  // src/bcon.cpp:22
@@ -697,23 +748,18 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
         upload_lines(g, st);
         if (g->fp32) {
             upload_background(g, st);
-            std::vector<double> R, T;
-            background_columns(g, R, T);
-            const int64_t NX = d.nx, NY = d.ny, NZ = d.nz, per = NX * NY;
-            std::vector<float> tmp((size_t)(per * NZ));
+            // each field: one contiguous FP64 copy into a staging buffer, then the deviation from
+            // the background and the rounding to FP32 on the device
+            Fp64Staging stg(g);
             for (int q = 0; q < 5; ++q) {
-                for (int64_t k = 0; k < NZ; ++k) {
-                    const double bgv = q == 3 ? R[k] : (q == 4 ? T[k] : 0.0);
-                    const double* a = src[q] + k * per;
-                    float* o = tmp.data() + k * per;
-                    for (int64_t n = 0; n < per; ++n) o[n] = (float)(a[n] - bgv);
-                }
-                cuda_ok(cudaMemcpy2D(g->X32[0][q], g->geo.pitch * sizeof(float), tmp.data(), NX * sizeof(float),
-                                     NX * sizeof(float), NY * NZ, cudaMemcpyHostToDevice),
+                cuda_ok(cudaMemcpyAsync(stg.buf, src[q], stg.n * sizeof(double), cudaMemcpyHostToDevice, g->stream),
                         "upload state32");
+                to_fp32_kernel<<<stg.blocks(), 256, 0, g->stream>>>(g->X32[0][q], g->geo.pitch, g->geo.plane, stg.buf,
+                                                                    d.nx, d.ny, d.nz, stg.bg(q));
+                cuda_ok(cudaGetLastError(), "upload state32");
                 // the second buffer gets the same contents on the device (its z ghost planes are
                 // never written by a stage)
-                cuda_ok(cudaMemcpyAsync(g->X32[1][q], g->X32[0][q], (size_t)g->geo.plane * NZ * sizeof(float),
+                cuda_ok(cudaMemcpyAsync(g->X32[1][q], g->X32[0][q], (size_t)g->geo.plane * d.nz * sizeof(float),
                                         cudaMemcpyDeviceToDevice, g->stream),
                         "upload state32");
             }
@@ -762,21 +808,16 @@ int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc) {
         const Derived& d = g->d;
         double* dst[r3dk::kMaxFields] = {st->ru, st->rv, st->rw, st->ro, st->tt, st->bx, st->by, st->bz};
         if (g->fp32) {
-            std::vector<double> R, T;
-            background_columns(g, R, T);
-            const int64_t NX = d.nx, NY = d.ny, NZ = d.nz, per = NX * NY;
-            std::vector<float> tmp((size_t)(per * NZ));
-            cuda_ok(cudaStreamSynchronize(g->stream), "download");
+            Fp64Staging stg(g);
             for (int q = 0; q < 5; ++q) {
                 if (!dst[q]) continue;
-                cuda_ok(cudaMemcpy2D(tmp.data(), NX * sizeof(float), g->X32[g->cur][q], g->geo.pitch * sizeof(float),
-                                     NX * sizeof(float), NY * NZ, cudaMemcpyDeviceToHost),
+                from_fp32_kernel<<<stg.blocks(), 256, 0, g->stream>>>(stg.buf, g->X32[g->cur][q], g->geo.pitch,
+                                                                      g->geo.plane, d.nx, d.ny, d.nz, stg.bg(q));
+                cuda_ok(cudaGetLastError(), "download state32");
+                cuda_ok(cudaMemcpyAsync(dst[q], stg.buf, stg.n * sizeof(double), cudaMemcpyDeviceToHost, g->stream),
                         "download state32");
-                for (int64_t k = 0; k < NZ; ++k) {
-                    const double bgv = q == 3 ? R[k] : (q == 4 ? T[k] : 0.0);
-                    for (int64_t n = 0; n < per; ++n) dst[q][k * per + n] = bgv + (double)tmp[k * per + n];
-                }
             }
+            cuda_ok(cudaStreamSynchronize(g->stream), "download state32");
         } else {
             for (int q = 0; q < g->nfields; ++q) {
                 if (!dst[q]) continue;
