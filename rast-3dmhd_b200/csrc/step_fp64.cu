@@ -38,6 +38,9 @@
 #ifndef R3D_STAGE_TY
 #define R3D_STAGE_TY 8
 #endif
+#ifndef R3D_STAGE_CPT
+#define R3D_STAGE_CPT 2
+#endif
 
 namespace r3dk {
 
@@ -49,6 +52,21 @@ enum { R_RU, R_RV, R_RW, R_RO, R_TT, R_BX, R_BY, R_BZ };
 enum { D_U, D_V, D_W, D_P, D_RI, D_NF };
 constexpr int NRAW = 4, NDER = 4;
 
+// Cells per thread: a hydro thread computes CPT adjacent rows of its tile column, so each warp
+// carries CPT independent stencil evaluations (and shares the y-neighbour loads between them);
+// an MHD cell already needs most of the register file, so MHD threads take one row.
+template <bool B>
+struct EdgeTag {
+    static constexpr bool value = B;
+};
+
+template <bool MHD>
+struct Cells {
+    static constexpr int cpt = MHD ? 1 : R3D_STAGE_CPT;
+    static constexpr int nt = TX * TY / cpt;  // threads per CTA
+    static_assert(TY % cpt == 0, "tile rows must divide among the threads");
+};
+
 template <bool MHD>
 struct Shape {
     static constexpr int nf = MHD ? 8 : 5;                 // raw fields per plane
@@ -58,7 +76,7 @@ struct Shape {
     static constexpr size_t der_bytes = (size_t)NDER * der_slot * sizeof(double);
     static constexpr uint32_t plane_tx = nf * SN * sizeof(double);  // TMA bytes per plane
     static constexpr size_t smem = raw_bytes + der_bytes + 64;
-    static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && NT <= 256) ? 2 : 1;
+    static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && Cells<MHD>::nt <= 256) ? 2 : 1;
     static_assert(raw_bytes % 128 == 0 && (RAWF * 8) % 128 == 0, "TMA destinations 128-byte aligned");
 };
 }  // namespace
@@ -70,11 +88,12 @@ void stage_fp64_box(unsigned* bx, unsigned* by) {
 }
 
 template <int STAGE, bool KC, bool MHD, bool EMIT>
-__global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
+__global__ void __launch_bounds__(Cells<MHD>::nt, Shape<MHD>::min_blocks)
     stage_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
                FieldSet fs, Scalars* sc, int kchunk) {
     using S = Shape<MHD>;
     constexpr int NF = S::nf;
+    constexpr int CPT = Cells<MHD>::cpt, NTH = Cells<MHD>::nt;
     extern __shared__ __align__(128) unsigned char smem[];
     double* raw = reinterpret_cast<double*>(smem);
     double* der = reinterpret_cast<double*>(smem + S::raw_bytes);
@@ -87,9 +106,7 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
     const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
     const int kb = 1 + blockIdx.z * kchunk;
     const int ke = min(g.npz, kb + kchunk - 1);
-    const int i = i0 + tx, j = j0 + ty;
-    const bool active = (i <= g.npx) && (j <= g.npy);
-    const int s0 = (ty + 1) * SX + (tx + 1);
+    const int i = i0 + tx, jr = j0 + ty * CPT;  // the thread's column and first row
 
     // plane p has local index q = p - (kb - 1); ring slot q % 4, mbarrier phase (q / 4) & 1
     int last_issued = kb - 2, last_waited = kb - 2;  // bookkeeping of thread 0 for the drain
@@ -109,7 +126,7 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
         last_waited = p;
         const double* r = raw + (q % NRAW) * S::raw_slot;
         double* d = der + (q % NDER) * S::der_slot;
-        for (int c = tid; c < SN; c += NT) {
+        for (int c = tid; c < SN; c += NTH) {
             const double ro = r[R_RO * RAWF + c];
             const double ri = __drcp_rn(ro);  // == 1.0/ro, src/fluxes.cpp:137
             d[D_U * SN + c] = r[R_RU * RAWF + c] * ri;          // src/fluxes.cpp:158
@@ -149,37 +166,44 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
     const double cg = ph.gam[STAGE] * dt;
     const double cz = (STAGE < 2) ? ph.zeta[STAGE + 1] * dt : 0.0;
     const double hx = ph.hx, h2x = ph.h2x, hy = ph.hy, hz = ph.hz;
-    const int ia = active ? i : 1, ja = active ? j : 1;
+    const int ia = (i <= g.npx) ? i : 1;
     const double dx1 = L.dxxdx[ia], d2x = L.d2xxdx2[ia];
-    const double dyj = L.dyydy[ja], tmpy = L.tmpy[ja], tmpy1 = L.tmpy1[ja], tmpy2 = L.tmpy2[ja];
-
     // 32-bit element offsets (a field holds < 2^31 elements, checked at create)
     const int PL = (int)g.plane, PX = (int)g.pitch;
-    const int col = ja * PX + ia;
     // offsets from a cell to its periodic ghost images (0: none)
     const int gdx = (i == 1) ? g.npx : ((i == g.npx) ? -g.npx : 0);
-    const int gdy = (j == 1) ? g.npy * PX : ((j == g.npy) ? -g.npy * PX : 0);
-    const bool ghost = active && (gdx != 0 || gdy != 0);
 
-    // RK accumulator Z of the thread's own cell, loaded one plane ahead (registers)
-    double zn[NF];
+    // per row c of the thread: activity, y metrics, column offset, and the RK accumulator Z of
+    // the cell, loaded one plane ahead (registers)
+    bool actv[CPT];
+    int colv[CPT];
+    double zn[CPT][NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) zn[f] = 0.0;
-    if (STAGE > 0 && active) {
+    for (int c = 0; c < CPT; ++c) {
+        const int j = jr + c;
+        actv[c] = (i <= g.npx) && (j <= g.npy);
+        colv[c] = ((j <= g.npy) ? j : 1) * PX + ia;
 #pragma unroll
-        for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][kb * PL + col];
+        for (int f = 0; f < NF; ++f) zn[c][f] = 0.0;
+        if (STAGE > 0 && actv[c]) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) zn[c][f] = fs.z[f][kb * PL + colv[c]];
+        }
     }
 
     for (int k = kb; k <= ke; ++k) {
         const int q = k - (kb - 1);
         // the next plane's accumulators: issued before the derive phase and the barrier, so
         // their latency hides behind a whole plane of work
-        double zq[NF];
+        double zq[CPT][NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) zq[f] = zn[f];
-        if (STAGE > 0 && active && k < ke) {
+        for (int c = 0; c < CPT; ++c) {
 #pragma unroll
-            for (int f = 0; f < NF; ++f) zn[f] = fs.z[f][(k + 1) * PL + col];
+            for (int f = 0; f < NF; ++f) zq[c][f] = zn[c][f];
+            if (STAGE > 0 && actv[c] && k < ke) {
+#pragma unroll
+                for (int f = 0; f < NF; ++f) zn[c][f] = fs.z[f][(k + 1) * PL + colv[c]];
+            }
         }
         if (!derive(k + 1)) s_abort = 1;
         __syncthreads();
@@ -188,26 +212,40 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
             fence_proxy_async();
             issue(k + 2);
         }
-        if (active) {
-            const int nc = k * PL + col;
-            const double* rm = raw + ((q + NRAW - 1) % NRAW) * S::raw_slot;
-            const double* r0 = raw + (q % NRAW) * S::raw_slot;
-            const double* rp = raw + ((q + 1) % NRAW) * S::raw_slot;
-            const double* dm = der + ((q + NDER - 1) % NDER) * S::der_slot;
-            const double* d0 = der + (q % NDER) * S::der_slot;
-            const double* dp = der + ((q + 1) % NDER) * S::der_slot;
+        const double* rm = raw + ((q + NRAW - 1) % NRAW) * S::raw_slot;
+        const double* r0 = raw + (q % NRAW) * S::raw_slot;
+        const double* rp = raw + ((q + 1) % NRAW) * S::raw_slot;
+        const double* dm = der + ((q + NDER - 1) % NDER) * S::der_slot;
+        const double* d0 = der + (q % NDER) * S::der_slot;
+        const double* dp = der + ((q + 1) % NDER) * S::der_slot;
 #define RW_(P, F, DX, DY) P[(F)*RAWF + s0 + (DY)*SX + (DX)]
 #define DV_(P, F, DX, DY) P[(F)*SN + s0 + (DY)*SX + (DX)]
-            const double tmpz = L.tmpz[k];
-            const bool edge = (k == 1 && g.top_edge) || (k == g.npz && g.bot_edge);
+        const double tmpz = L.tmpz[k];
+        const bool edge = (k == 1 && g.top_edge) || (k == g.npz && g.bot_edge);
+        // right-hand sides of the thread's cells: all rows first, so that their independent
+        // stencil evaluations can interleave, then the stage updates and stores
+        double Fc[CPT][NF];
+        // the plane's edge status is uniform over the CTA: one straight-line copy of the stencil
+        // per case, so that the rows' evaluations share basic blocks
+        auto rhs = [&](auto edge_tag) {
+          constexpr bool EDGE = decltype(edge_tag)::value;
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) Fc[c][f] = 0.0;
+            const int j = jr + c, ja = (j <= g.npy) ? j : 1;
+            const int s0 = (ty * CPT + c + 1) * SX + (tx + 1);
+            const int nc = k * PL + colv[c];
+            const double dyj = L.dyydy[ja], tmpy = L.tmpy[ja], tmpy1 = L.tmpy1[ja], tmpy2 = L.tmpy2[ja];
+            // inactive rows (beyond a ragged tile edge) compute on in-bounds data and are not stored
 
             // ---- continuity, src/fluxes.cpp:87-121 ----
             double fr = (RW_(r0, R_RU, -1, 0) - RW_(r0, R_RU, 1, 0)) * hx * dx1;
             fr -= (RW_(r0, R_RV, 0, 1) - RW_(r0, R_RV, 0, -1)) * tmpy;
             double dwz;
-            if (k == 1 && g.top_edge)
+            if (EDGE && k == 1 && g.top_edge)
                 dwz = (4.0 * RW_(rp, R_RW, 0, 0) - fs.xin[R_RW][nc + 2 * PL]) * tmpz;
-            else if (k == g.npz && g.bot_edge)
+            else if (EDGE && k == g.npz && g.bot_edge)
                 dwz = (fs.xin[R_RW][nc - 2 * PL] - 4.0 * RW_(rm, R_RW, 0, 0)) * tmpz;
             else
                 dwz = (RW_(rp, R_RW, 0, 0) - RW_(rm, R_RW, 0, 0)) * tmpz;
@@ -238,7 +276,7 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
             const double vz = (Vzp - Vzm) * hz * dzk;  // :469; 3dmhdsub.f:2217
             const double wz = (Wzp - Wzm) * hz * dzk;  // :423; 3dmhdsub.f:2223
 
-            if (!edge) {
+            if (!EDGE) {
                 const double tmpz1 = L.tmpz1[k], tmpz2 = L.tmpz2[k];
                 const double T0 = RW_(r0, R_TT, 0, 0);
 
@@ -326,7 +364,7 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 ft += 2.0 * uz * wx * ri * th;  // :513
 
                 // ---- rotation, src/fluxes.cpp:519-533 ----
-                if (ph.lrot) {
+                if (MHD && ph.lrot) {  // hydro: added before the stage update
                     fu += ph.omz * RW_(r0, R_RV, 0, 0);
                     fv += -ph.omz * RW_(r0, R_RU, 0, 0) + ph.omx * RW_(r0, R_RW, 0, 0);
                     fw += -ph.omx * RW_(r0, R_RV, 0, 0);
@@ -351,11 +389,11 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 const double BZzp = RW_(rp, R_BZ, 0, 0), BZzm = RW_(rm, R_BZ, 0, 0);
                 // dW/dz with the one-sided forms at the top and bottom planes (2245-2259)
                 double wzb = wz;
-                if (k == 1 && g.top_edge) {
+                if (EDGE && k == 1 && g.top_edge) {
                     const int n2 = nc + 2 * PL;
                     const double w2 = fs.xin[R_RW][n2] * __drcp_rn(fs.xin[R_RO][n2]);
                     wzb = (4.0 * Wzp - w2) * hz * dzk;
-                } else if (k == g.npz && g.bot_edge) {
+                } else if (EDGE && k == g.npz && g.bot_edge) {
                     const int n2 = nc - 2 * PL;
                     const double w2 = fs.xin[R_RW][n2] * __drcp_rn(fs.xin[R_RO][n2]);
                     wzb = (w2 - 4.0 * Wzm) * hz * dzk;
@@ -392,14 +430,14 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 b1 = b1 - W0 * bxz;                        // 1370
                 b2f = b2f - V0 * byy;                      // 1380
                 double d2bxz, d2byz;
-                if (k == 1 && g.top_edge) {  // 1391, 1511
+                if (EDGE && k == 1 && g.top_edge) {  // 1391, 1511
                     const double bx2 = fs.xin[R_BX][nc + 2 * PL], bx3 = fs.xin[R_BX][nc + 3 * PL];
                     const double by2 = fs.xin[R_BY][nc + 2 * PL], by3 = fs.xin[R_BY][nc + 3 * PL];
                     d2bxz = (-3.0 * BX0 + 4.0 * BXzp - bx2) * hz * d2z +
                             (2.0 * BX0 - 5.0 * BXzp + 4.0 * bx2 - bx3) * h2z * dzk * dzk;
                     d2byz = (-3.0 * BY0 + 4.0 * BYzp - by2) * hz * d2z +
                             (2.0 * BY0 - 5.0 * BYzp + 4.0 * by2 - by3) * h2z * dzk * dzk;
-                } else if (k == g.npz && g.bot_edge) {  // 1392, 1513
+                } else if (EDGE && k == g.npz && g.bot_edge) {  // 1392, 1513
                     const double bx2 = fs.xin[R_BX][nc - 2 * PL], bx3 = fs.xin[R_BX][nc - 3 * PL];
                     const double by2 = fs.xin[R_BY][nc - 2 * PL], by3 = fs.xin[R_BY][nc - 3 * PL];
                     d2bxz = (3.0 * BX0 - 4.0 * BXzm + bx2) * hz * d2z +
@@ -428,27 +466,43 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                 b3 = b3 - W0 * bzz;                        // 1560
                 const double d2bzz = (BZzp - BZzm) * hz * d2z + (BZzp - 2.0 * BZ0 + BZzm) * h2z * dzk * dzk;  // 1570
                 b3 = b3 + orm * d2bzz;                     // 1580
-                if (edge) {  // the hydro fluxes there are rewritten by BCON: keep them finite
+                if (EDGE) {  // the hydro fluxes there are rewritten by BCON: keep them finite
                     fu = fv = fw = ft = 0.0;
                 }
             }
-
-            // ---- stage update, src/step.cpp:53-110 (B: 3dmhdsub.f:957-973, 1059-1075, 1161-1177) ----
-            double F[NF];
-            F[0] = fu;
-            F[1] = fv;
-            F[2] = fw;
-            F[3] = fr;
-            F[4] = ft;
+            Fc[c][0] = fu;
+            Fc[c][1] = fv;
+            Fc[c][2] = fw;
+            Fc[c][3] = fr;
+            Fc[c][4] = ft;
             if constexpr (MHD) {
-                F[5] = b1;
-                F[6] = b2f;
-                F[7] = b3;
+                Fc[c][5] = b1;
+                Fc[c][6] = b2f;
+                Fc[c][7] = b3;
             }
+          }
+        };
+        if (edge) rhs(EdgeTag<true>{});
+        else rhs(EdgeTag<false>{});
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          if (actv[c]) {
+            // ---- stage update, src/step.cpp:53-110 (B: 3dmhdsub.f:957-973, 1059-1075, 1161-1177) ----
+            const int j = jr + c;
+            const int s0 = (ty * CPT + c + 1) * SX + (tx + 1);
+            const int nc = k * PL + colv[c];
+            double* F = Fc[c];
+            if (!MHD && !edge && ph.lrot) {  // rotation, src/fluxes.cpp:519-533 (the last terms)
+                F[0] += ph.omz * RW_(r0, R_RV, 0, 0);
+                F[1] += -ph.omz * RW_(r0, R_RU, 0, 0) + ph.omx * RW_(r0, R_RW, 0, 0);
+                F[2] += -ph.omx * RW_(r0, R_RV, 0, 0);
+            }
+            const int gdy = (j == 1) ? g.npy * PX : ((j == g.npy) ? -g.npy * PX : 0);
+            const bool ghost = gdx != 0 || gdy != 0;
             double xn[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
-                const double zv = (STAGE == 0) ? RW_(r0, f, 0, 0) : zq[f];
+                const double zv = (STAGE == 0) ? RW_(r0, f, 0, 0) : zq[c][f];
                 xn[f] = zv + cg * F[f];
                 fs.xout[f][nc] = xn[f];
                 if (STAGE < 2) fs.z[f][nc] = xn[f] + cz * F[f];
@@ -480,9 +534,10 @@ __global__ void __launch_bounds__(NT, Shape<MHD>::min_blocks)
                     mu = fold_max(mu, um);
                 }
             }
+          }
+        }
 #undef RW_
 #undef DV_
-        }
     }
     __syncthreads();
     if (s_abort) {
@@ -515,7 +570,7 @@ static void launch_one(dim3 grid, dim3 block, const StageMaps& maps, const Geome
 template <bool MHD, bool EMIT>
 static void launch_stage(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                          const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
-    dim3 block(TX, TY, 1);
+    dim3 block(TX, TY / Cells<MHD>::cpt, 1);
     dim3 grid((g.npx + TX - 1) / TX, (g.npy + TY - 1) / TY, (g.npz + kchunk - 1) / kchunk);
     const bool kc = ph.kappa_const != 0;
     if (stage == 0) kc ? launch_one<0, true, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
