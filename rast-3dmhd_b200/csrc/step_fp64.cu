@@ -38,8 +38,14 @@
 #ifndef R3D_STAGE_TY
 #define R3D_STAGE_TY 8
 #endif
-#ifndef R3D_STAGE_CPT
-#define R3D_STAGE_CPT 2
+#ifndef R3D_CPT_S0
+#define R3D_CPT_S0 2
+#endif
+#ifndef R3D_CPT_S1
+#define R3D_CPT_S1 2
+#endif
+#ifndef R3D_CPT_S2
+#define R3D_CPT_S2 1  // the third stage's dt epilogue runs better with one row per thread
 #endif
 
 namespace r3dk {
@@ -53,16 +59,17 @@ enum { D_U, D_V, D_W, D_P, D_RI, D_NF };
 constexpr int NRAW = 4, NDER = 4;
 
 // Cells per thread: a hydro thread computes CPT adjacent rows of its tile column, so each warp
-// carries CPT independent stencil evaluations (and shares the y-neighbour loads between them);
-// an MHD cell already needs most of the register file, so MHD threads take one row.
+// carries CPT independent stencil evaluations (and shares the y-neighbour loads between them).
+// Two rows in the first two stages, one in the third (its filtered dt epilogue branches per
+// cell); an MHD cell already needs most of the register file, so MHD threads take one row.
 template <bool B>
 struct EdgeTag {
     static constexpr bool value = B;
 };
 
-template <bool MHD>
+template <bool MHD, int STAGE>
 struct Cells {
-    static constexpr int cpt = MHD ? 1 : R3D_STAGE_CPT;
+    static constexpr int cpt = MHD ? 1 : (STAGE == 0 ? R3D_CPT_S0 : (STAGE == 1 ? R3D_CPT_S1 : R3D_CPT_S2));
     static constexpr int nt = TX * TY / cpt;  // threads per CTA
     static_assert(TY % cpt == 0, "tile rows must divide among the threads");
 };
@@ -76,7 +83,7 @@ struct Shape {
     static constexpr size_t der_bytes = (size_t)NDER * der_slot * sizeof(double);
     static constexpr uint32_t plane_tx = nf * SN * sizeof(double);  // TMA bytes per plane
     static constexpr size_t smem = raw_bytes + der_bytes + 64;
-    static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && Cells<MHD>::nt <= 256) ? 2 : 1;
+    static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && TX * TY <= 256) ? 2 : 1;
     static_assert(raw_bytes % 128 == 0 && (RAWF * 8) % 128 == 0, "TMA destinations 128-byte aligned");
 };
 }  // namespace
@@ -88,12 +95,12 @@ void stage_fp64_box(unsigned* bx, unsigned* by) {
 }
 
 template <int STAGE, bool KC, bool MHD, bool EMIT>
-__global__ void __launch_bounds__(Cells<MHD>::nt, Shape<MHD>::min_blocks)
+__global__ void __launch_bounds__(Cells<MHD, STAGE>::nt, Shape<MHD>::min_blocks)
     stage_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
                FieldSet fs, Scalars* sc, int kchunk) {
     using S = Shape<MHD>;
     constexpr int NF = S::nf;
-    constexpr int CPT = Cells<MHD>::cpt, NTH = Cells<MHD>::nt;
+    constexpr int CPT = Cells<MHD, STAGE>::cpt, NTH = Cells<MHD, STAGE>::nt;
     extern __shared__ __align__(128) unsigned char smem[];
     double* raw = reinterpret_cast<double*>(smem);
     double* der = reinterpret_cast<double*>(smem + S::raw_bytes);
@@ -564,13 +571,14 @@ static void launch_one(dim3 grid, dim3 block, const StageMaps& maps, const Geome
         cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         configured = true;
     }
+    block.y = TY / Cells<MHD, STAGE>::cpt;
     stage_fp64<STAGE, KC, MHD, EMIT><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
 }
 
 template <bool MHD, bool EMIT>
 static void launch_stage(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                          const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
-    dim3 block(TX, TY / Cells<MHD>::cpt, 1);
+    dim3 block(TX, TY, 1);  // rows per thread set per stage in launch_one
     dim3 grid((g.npx + TX - 1) / TX, (g.npy + TY - 1) / TY, (g.npz + kchunk - 1) / kchunk);
     const bool kc = ph.kappa_const != 0;
     if (stage == 0) kc ? launch_one<0, true, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
