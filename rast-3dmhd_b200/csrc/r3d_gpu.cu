@@ -614,7 +614,7 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
                         g->bytes += nbytes;
                     }
                 unsigned bx = 0, by = 0;
-                r3dk::stage_fp64_box(&bx, &by);  // the box the stage kernel expects per plane
+                r3dk::stage_fp64_box(p->lmag, &bx, &by);  // the box the stage kernel expects per plane
                 for (int b = 0; b < 2; ++b)
                     for (int q = 0; q < g->nfields; ++q)
                         g->maps[b].m[q] = field_map(g->X[b][q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
@@ -654,17 +654,19 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             g->kchunk = R3D_KCHUNK;
 #else
             g->kchunk = nloc >= 512 ? 64 : (nloc >= 256 ? 32 : 16);
+            // column tiles of the stage kernel (32 x rows) and its resident CTAs per SM
+            unsigned tbx = 0, tby = 0;
+            if (g->fp32) r3dk::stage_fp32_box(&tbx, &tby);
+            else r3dk::stage_fp64_box(p->lmag, &tbx, &tby);
+            const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + (int)tby - 3) / ((int)tby - 2));
+            const int64_t slots = 148 * (g->fp32 ? 3 : 2);
             if (p->lmag) {
-                // one CTA per SM: prefer enough z-chunks for >= 8 full waves over 148 SMs
-                const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + 7) / 8);
-                while (g->kchunk > 16 && tiles * ((nloc + g->kchunk - 1) / g->kchunk) < 8 * 148) g->kchunk /= 2;
+                // few, heavy CTAs: prefer enough z-chunks for >= 4 full waves
+                while (g->kchunk > 16 && tiles * ((nloc + g->kchunk - 1) / g->kchunk) < 4 * slots) g->kchunk /= 2;
             }
             {
-                // small grids, whose launch does not fill the GPU once (resident CTAs per SM: 1 MHD,
-                // 2 FP64 hydro, 3 FP32-bulk): the chunk depth (down to 4) that minimises
-                // waves x (planes loaded per chunk)
-                const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + 7) / 8);
-                const int64_t slots = 148 * (p->lmag ? 1 : (g->fp32 ? 3 : 2));
+                // small grids, whose launch does not fill the GPU once: the chunk depth (down to 4)
+                // that minimises waves x (planes loaded per chunk)
                 auto ctas = [&](int k) { return tiles * ((nloc + k - 1) / k); };
                 auto cost = [&](int k) { return (ctas(k) + slots - 1) / slots * (k + 2); };
                 if (ctas(g->kchunk) < slots) {

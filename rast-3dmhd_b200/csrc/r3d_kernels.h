@@ -61,7 +61,7 @@ cudaError_t launch_totals_fp32(const Geometry& g, const Physics& ph, const Backg
 
 size_t stage_fp64_smem();
 // TMA box (x, y) of one field plane that the FP64 stage kernel was compiled for.
-void stage_fp64_box(unsigned* bx, unsigned* by);
+void stage_fp64_box(int mhd, unsigned* bx, unsigned* by);
 cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
                               const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
                               int kchunk, cudaStream_t st, bool emit_rhs = false);

@@ -13,7 +13,8 @@
 // and the B fluxes WW1..WW3) receives its terms in the reference's order, so with FMA
 // contraction off (-fmad=false) the result is bit-identical.
 //
-// Pipeline: a CTA owns a 32 x TY column tile and marches down a chunk of z planes.  Thread 0
+// Pipeline: a CTA owns a 32 x TY column tile (TY = 8 hydro, 6 MHD) and marches down a chunk of
+// z planes.  Thread 0
 // streams the state fields of each plane, with a one-cell x/y halo, into a 4-slot ring by TMA
 // (one (34, TY+2, 1) box per field, completion on a per-slot mbarrier), two planes ahead of
 // the plane being computed.  Each loaded cell is then turned once into 1/rho, u, v, w and
@@ -36,7 +37,10 @@
 #include "tma.cuh"
 
 #ifndef R3D_STAGE_TY
-#define R3D_STAGE_TY 8
+#define R3D_STAGE_TY 8  // tile rows, hydro
+#endif
+#ifndef R3D_STAGE_TY_MHD
+#define R3D_STAGE_TY_MHD 6  // tile rows, MHD: two 192-thread CTAs per SM fit beside the 8-field rings
 #endif
 #ifndef R3D_CPT_S0
 #define R3D_CPT_S0 2
@@ -51,9 +55,7 @@
 namespace r3dk {
 
 namespace {
-constexpr int TX = 32, TY = R3D_STAGE_TY, NT = TX * TY;
-constexpr int SX = TX + 2, SY = TY + 2, SN = SX * SY;  // cells per halo tile
-constexpr int RAWF = (SN + 15) / 16 * 16;  // doubles per raw field box, 128 B multiple
+constexpr int TX = 32, SX = TX + 2;
 enum { R_RU, R_RV, R_RW, R_RO, R_TT, R_BX, R_BY, R_BZ };
 enum { D_U, D_V, D_W, D_P, D_RI, D_NF };
 constexpr int NRAW = 4, NDER = 4;
@@ -67,31 +69,34 @@ struct EdgeTag {
     static constexpr bool value = B;
 };
 
+template <bool MHD>
+struct Shape {
+    static constexpr int ty = MHD ? R3D_STAGE_TY_MHD : R3D_STAGE_TY;  // tile rows
+    static constexpr int sy = ty + 2, sn = SX * sy;                     // cells per halo tile
+    static constexpr int rawf = (sn + 15) / 16 * 16;  // doubles per raw field box, 128 B multiple
+    static constexpr int nf = MHD ? 8 : 5;                 // raw fields per plane
+    static constexpr int raw_slot = nf * rawf;             // doubles
+    static constexpr int der_slot = D_NF * sn;             // doubles
+    static constexpr size_t raw_bytes = (size_t)NRAW * raw_slot * sizeof(double);
+    static constexpr size_t der_bytes = (size_t)NDER * der_slot * sizeof(double);
+    static constexpr uint32_t plane_tx = nf * sn * sizeof(double);  // TMA bytes per plane
+    static constexpr size_t smem = raw_bytes + der_bytes + 64;
+    static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && TX * ty <= 256) ? 2 : 1;
+    static_assert(raw_bytes % 128 == 0 && (rawf * 8) % 128 == 0, "TMA destinations 128-byte aligned");
+};
+
 template <bool MHD, int STAGE>
 struct Cells {
     static constexpr int cpt = MHD ? 1 : (STAGE == 0 ? R3D_CPT_S0 : (STAGE == 1 ? R3D_CPT_S1 : R3D_CPT_S2));
-    static constexpr int nt = TX * TY / cpt;  // threads per CTA
-    static_assert(TY % cpt == 0, "tile rows must divide among the threads");
-};
-
-template <bool MHD>
-struct Shape {
-    static constexpr int nf = MHD ? 8 : 5;                 // raw fields per plane
-    static constexpr int raw_slot = nf * RAWF;             // doubles
-    static constexpr int der_slot = D_NF * SN;             // doubles
-    static constexpr size_t raw_bytes = (size_t)NRAW * raw_slot * sizeof(double);
-    static constexpr size_t der_bytes = (size_t)NDER * der_slot * sizeof(double);
-    static constexpr uint32_t plane_tx = nf * SN * sizeof(double);  // TMA bytes per plane
-    static constexpr size_t smem = raw_bytes + der_bytes + 64;
-    static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && TX * TY <= 256) ? 2 : 1;
-    static_assert(raw_bytes % 128 == 0 && (RAWF * 8) % 128 == 0, "TMA destinations 128-byte aligned");
+    static constexpr int nt = TX * Shape<MHD>::ty / cpt;  // threads per CTA
+    static_assert(Shape<MHD>::ty % cpt == 0, "tile rows must divide among the threads");
 };
 }  // namespace
 
 size_t stage_fp64_smem() { return Shape<false>::smem; }
-void stage_fp64_box(unsigned* bx, unsigned* by) {
+void stage_fp64_box(int mhd, unsigned* bx, unsigned* by) {
     *bx = SX;
-    *by = SY;
+    *by = mhd ? Shape<true>::sy : Shape<false>::sy;
 }
 
 template <int STAGE, bool KC, bool MHD, bool EMIT>
@@ -100,6 +105,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE>::nt, Shape<MHD>::min_blocks)
                FieldSet fs, Scalars* sc, int kchunk) {
     using S = Shape<MHD>;
     constexpr int NF = S::nf;
+    constexpr int TY = S::ty, SN = S::sn, RAWF = S::rawf;
     constexpr int CPT = Cells<MHD, STAGE>::cpt, NTH = Cells<MHD, STAGE>::nt;
     extern __shared__ __align__(128) unsigned char smem[];
     double* raw = reinterpret_cast<double*>(smem);
@@ -571,13 +577,14 @@ static void launch_one(dim3 grid, dim3 block, const StageMaps& maps, const Geome
         cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         configured = true;
     }
-    block.y = TY / Cells<MHD, STAGE>::cpt;
+    block.y = Shape<MHD>::ty / Cells<MHD, STAGE>::cpt;
     stage_fp64<STAGE, KC, MHD, EMIT><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
 }
 
 template <bool MHD, bool EMIT>
 static void launch_stage(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                          const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
+    constexpr int TY = Shape<MHD>::ty;
     dim3 block(TX, TY, 1);  // rows per thread set per stage in launch_one
     dim3 grid((g.npx + TX - 1) / TX, (g.npy + TY - 1) / TY, (g.npz + kchunk - 1) / kchunk);
     const bool kc = ph.kappa_const != 0;

@@ -130,6 +130,26 @@ def test_graph_replay_matches_step_loop(flags, lead):
 
 
 @pytest.mark.gpu
+def test_graph_replay_survives_reupload_and_enqueue():
+    """The captured step graph keeps working after a new upload (same buffers, new contents) and
+    through r3d_gpu_enqueue: the result equals a fresh handle's step loop."""
+    flags = ["--npx", "40", "--npy", "24", "--npz", "48", "--seed", "4"]
+    p = R.parse(flags)
+    ref, sref = gpu_run(flags[:-2], 4, 6)
+    st = R.HostState.setup(p)
+    with R.GpuSim(p) as sim:
+        sim.upload(st)
+        sim.run(6)                      # captures the graph on other contents
+        sim.upload(st)                  # back to the initial state
+        sim.enqueue(4)
+        sc = sim.run(2)
+        sim.download(st)
+    for n in PRIMARY:
+        assert np.array_equal(interior(st.fields[n]), interior(ref.fields[n])), n
+    assert sc == sref
+
+
+@pytest.mark.gpu
 def test_gpu_vs_reference_build_directly():
     """When the reference CPU build is present, also compare against it without the oracle."""
     if not Reference.available():
