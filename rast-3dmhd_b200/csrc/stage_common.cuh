@@ -73,13 +73,15 @@ __device__ __forceinline__ void fold_dt_filtered(const Physics& ph, double ru, d
     const float umf = __fdividef(ph.ogamma_f * uuf, ttf);
     const float gtf = ph.gamma_f * ttf;
     float c2f;
+    // square roots as x * rsqrt(x) (2 ulp each; 0 for x == 0)
+    auto sqrt_est = [](float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; };
     if constexpr (MHD) {
         const float b2f = (float)b2sum * ph.obeta_f * rf;
-        c2f = uuf + gtf + b2f + 2.0f * sqrtf(uuf * (gtf + b2f));
+        c2f = uuf + gtf + b2f + 2.0f * sqrt_est(uuf * (gtf + b2f));
     } else {
-        c2f = uuf + gtf + 2.0f * sqrtf(uuf * gtf);
+        c2f = uuf + gtf + 2.0f * sqrt_est(uuf * gtf);
     }
-    const float w1f = __fdividef((float)dd, sqrtf(c2f));
+    const float w1f = (float)dd * rsqrtf(c2f);
     const double b1 = (t1 < m1) ? t1 : m1;
     const double bu = (mu < tu) ? tu : mu;
     const bool ok = est_window(ro) && est_window(tt) && est_window(dd);

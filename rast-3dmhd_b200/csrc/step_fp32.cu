@@ -328,9 +328,13 @@ __global__ void __launch_bounds__(NT, 3)
         }
         if (STAGE == 2 && !edge) {  // dt limits, FP64 values on full state (filtered)
             const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[k]);
-            fold_dt_filtered<false, false>(ph, xn[0], xn[1], xn[2], bg.r[k] + (double)xn[3],
-                                           bg.t[k] + (double)xn[4], 0.0, dd, L.rkapa[k], s_thr[0],
-                                           s_thr[1], m1, m2, m3, m4, mu);
+            const double ro = bg.r[k] + (double)xn[3], tt = bg.t[k] + (double)xn[4];
+            if (ph.kappa_const)  // rkapa == 1 on every plane: x/rkapa == x, no division
+                fold_dt_filtered<true, false>(ph, xn[0], xn[1], xn[2], ro, tt, 0.0, dd, 1.0, s_thr[0],
+                                              s_thr[1], m1, m2, m3, m4, mu);
+            else
+                fold_dt_filtered<false, false>(ph, xn[0], xn[1], xn[2], ro, tt, 0.0, dd, L.rkapa[k], s_thr[0],
+                                               s_thr[1], m1, m2, m3, m4, mu);
         }
 #undef RW_
 #undef DV_
