@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(NT, 3)
     const double cg = ph.gam[STAGE] * dt;
     const double cz = (STAGE < 2) ? ph.zeta[STAGE + 1] * dt : 0.0;
     const int ia = active ? i : 1, ja = active ? j : 1;
+    const double dxy = (L.ddy[ja] < L.ddx[ia]) ? L.ddy[ja] : L.ddx[ia];  // the plane-independent part of dd
     const float cx = (float)(ph.hx * L.dxxdx[ia]);                       // d/dx
     const float cx1 = (float)(ph.hx * L.d2xxdx2[ia]);                    // second-derivative parts
     const float cx2 = (float)(ph.h2x * L.dxxdx[ia] * L.dxxdx[ia]);
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(NT, 3)
             }
         }
         if (STAGE == 2 && !edge) {  // dt limits, FP64 values on full state (filtered)
-            const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[k]);
+            const double dd = (L.ddz[k] < dxy) ? L.ddz[k] : dxy;  // min_of3(ddx, ddy, ddz)
             const double ro = bg.r[k] + (double)xn[3], tt = bg.t[k] + (double)xn[4];
             if (ph.kappa_const)  // rkapa == 1 on every plane: x/rkapa == x, no division
                 fold_dt_filtered<true, false>(ph, xn[0], xn[1], xn[2], ro, tt, 0.0, dd, 1.0, s_thr[0],

@@ -191,11 +191,16 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE>::nt, Shape<MHD>::min_blocks)
     bool actv[CPT];
     int colv[CPT];
     double zn[CPT][NF];
+    double dxyv[CPT];  // third stage: min(ddx[i], ddy[j]), the plane-independent part of dd
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
         const int j = jr + c;
         actv[c] = (i <= g.npx) && (j <= g.npy);
         colv[c] = ((j <= g.npy) ? j : 1) * PX + ia;
+        if (STAGE == 2) {
+            const int ja = (j <= g.npy) ? j : 1;
+            dxyv[c] = (L.ddy[ja] < L.ddx[ia]) ? L.ddy[ja] : L.ddx[ia];
+        }
 #pragma unroll
         for (int f = 0; f < NF; ++f) zn[c][f] = 0.0;
         if (STAGE > 0 && actv[c]) {
@@ -530,7 +535,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE>::nt, Shape<MHD>::min_blocks)
                 }
             }
             if (STAGE == 2 && !edge) {
-                const double dd = min_of3(L.ddx[i], L.ddy[j], L.ddz[k]);
+                const double dd = (L.ddz[k] < dxyv[c]) ? L.ddz[k] : dxyv[c];  // min_of3(ddx, ddy, ddz)
                 double b2sum = 0.0;
                 if constexpr (MHD) b2sum = xn[5] * xn[5] + xn[6] * xn[6] + xn[7] * xn[7];
                 if (s_filter) {
