@@ -258,7 +258,7 @@ Adjoint* workspace(r3d_gpu* g) {
         A->field_elems = g->geo.plane * (g->geo.npz + 2);
         const size_t st = (size_t)A->nf * A->field_elems;
         unsigned bx = 0, by = 0;
-        r3dk::stage_fp64_box(g->p.lmag, &bx, &by);
+        r3dk::stage_fp64_box(g->geo.tile_rows, &bx, &by);
         for (int s = 0; s < 4; ++s) {
             A->S[s].base = dalloc(A, st);
             for (int f = 0; f < A->nf; ++f)

@@ -21,6 +21,7 @@ struct Geometry {
     int64_t plane;      // doubles per z plane
     int top_edge;       // local plane 1 is the domain's top plane (BCON, one-sided stencils)
     int bot_edge;       // local plane npz is the domain's bottom plane
+    int tile_rows;      // rows of the FP64 stage kernel's column tiles (stage_fp64_rows)
 };
 
 struct Physics {

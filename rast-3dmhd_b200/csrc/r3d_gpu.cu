@@ -576,6 +576,7 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             g->geo.npz = nloc;
             g->geo.top_edge = z0 == 0 ? 1 : 0;
             g->geo.bot_edge = z0 + nloc == p->npz ? 1 : 0;
+            g->geo.tile_rows = r3dk::stage_fp64_rows(p->lmag, p->npx, p->npy, nloc);
             g->dt_filter = z0 == 0 && nloc == p->npz;
             g->geo.pitch = (d.nx + 15) / 16 * 16;
             g->geo.plane = g->geo.pitch * d.ny;
@@ -614,7 +615,7 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
                         g->bytes += nbytes;
                     }
                 unsigned bx = 0, by = 0;
-                r3dk::stage_fp64_box(p->lmag, &bx, &by);  // the box the stage kernel expects per plane
+                r3dk::stage_fp64_box(g->geo.tile_rows, &bx, &by);  // the box the stage kernel expects per plane
                 for (int b = 0; b < 2; ++b)
                     for (int q = 0; q < g->nfields; ++q)
                         g->maps[b].m[q] = field_map(g->X[b][q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
@@ -657,9 +658,9 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             // column tiles of the stage kernel (32 x rows) and its resident CTAs per SM
             unsigned tbx = 0, tby = 0;
             if (g->fp32) r3dk::stage_fp32_box(&tbx, &tby);
-            else r3dk::stage_fp64_box(p->lmag, &tbx, &tby);
+            else r3dk::stage_fp64_box(g->geo.tile_rows, &tbx, &tby);
             const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + (int)tby - 3) / ((int)tby - 2));
-            const int64_t slots = 148 * (g->fp32 ? 3 : 2);
+            const int64_t slots = 148 * ((g->fp32 ? 3 : 2) - (p->lmag && tby == 10 ? 1 : 0));
             if (p->lmag) {
                 // few, heavy CTAs: prefer enough z-chunks for >= 4 full waves
                 while (g->kchunk > 16 && tiles * ((nloc + g->kchunk - 1) / g->kchunk) < 4 * slots) g->kchunk /= 2;

@@ -39,9 +39,9 @@
 #ifndef R3D_STAGE_TY
 #define R3D_STAGE_TY 8  // tile rows, hydro
 #endif
-#ifndef R3D_STAGE_TY_MHD
-#define R3D_STAGE_TY_MHD 6  // tile rows, MHD: two 192-thread CTAs per SM fit beside the 8-field rings
-#endif
+// MHD tiles have 6 rows (two 192-thread CTAs per SM fit beside the 8-field rings) or, on grids
+// too small to give every SM two CTAs, 8 rows (one 256-thread CTA per SM); Geometry::tile_rows
+// holds the handle's choice.
 #ifndef R3D_CPT_S0
 #define R3D_CPT_S0 2
 #endif
@@ -69,9 +69,9 @@ struct EdgeTag {
     static constexpr bool value = B;
 };
 
-template <bool MHD>
+template <bool MHD, int TYV>
 struct Shape {
-    static constexpr int ty = MHD ? R3D_STAGE_TY_MHD : R3D_STAGE_TY;  // tile rows
+    static constexpr int ty = TYV;  // tile rows
     static constexpr int sy = ty + 2, sn = SX * sy;                     // cells per halo tile
     static constexpr int rawf = (sn + 15) / 16 * 16;  // doubles per raw field box, 128 B multiple
     static constexpr int nf = MHD ? 8 : 5;                 // raw fields per plane
@@ -85,28 +85,33 @@ struct Shape {
     static_assert(raw_bytes % 128 == 0 && (rawf * 8) % 128 == 0, "TMA destinations 128-byte aligned");
 };
 
-template <bool MHD, int STAGE>
+template <bool MHD, int STAGE, int TYV>
 struct Cells {
     static constexpr int cpt = MHD ? 1 : (STAGE == 0 ? R3D_CPT_S0 : (STAGE == 1 ? R3D_CPT_S1 : R3D_CPT_S2));
-    static constexpr int nt = TX * Shape<MHD>::ty / cpt;  // threads per CTA
-    static_assert(Shape<MHD>::ty % cpt == 0, "tile rows must divide among the threads");
+    static constexpr int nt = TX * TYV / cpt;  // threads per CTA
+    static_assert(TYV % cpt == 0, "tile rows must divide among the threads");
 };
 }  // namespace
 
-size_t stage_fp64_smem() { return Shape<false>::smem; }
-void stage_fp64_box(int mhd, unsigned* bx, unsigned* by) {
+size_t stage_fp64_smem() { return Shape<false, R3D_STAGE_TY>::smem; }
+int stage_fp64_rows(int mhd, int npx, int npy, int nloc) {
+    if (!mhd) return R3D_STAGE_TY;
+    const long tiles6 = (long)((npx + TX - 1) / TX) * ((npy + 5) / 6);
+    return tiles6 * ((nloc + 15) / 16) >= 2 * 148 ? 6 : 8;
+}
+void stage_fp64_box(int rows, unsigned* bx, unsigned* by) {
     *bx = SX;
-    *by = mhd ? Shape<true>::sy : Shape<false>::sy;
+    *by = rows + 2;
 }
 
-template <int STAGE, bool KC, bool MHD, bool EMIT>
-__global__ void __launch_bounds__(Cells<MHD, STAGE>::nt, Shape<MHD>::min_blocks)
+template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV>
+__global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::min_blocks)
     stage_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
                FieldSet fs, Scalars* sc, int kchunk) {
-    using S = Shape<MHD>;
+    using S = Shape<MHD, TYV>;
     constexpr int NF = S::nf;
     constexpr int TY = S::ty, SN = S::sn, RAWF = S::rawf;
-    constexpr int CPT = Cells<MHD, STAGE>::cpt, NTH = Cells<MHD, STAGE>::nt;
+    constexpr int CPT = Cells<MHD, STAGE, TYV>::cpt, NTH = Cells<MHD, STAGE, TYV>::nt;
     extern __shared__ __align__(128) unsigned char smem[];
     double* raw = reinterpret_cast<double*>(smem);
     double* der = reinterpret_cast<double*>(smem + S::raw_bytes);
@@ -572,45 +577,48 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE>::nt, Shape<MHD>::min_blocks)
     if (STAGE == 2) reduce_dt(der, m1, m2, m3, m4, mu, sc);
 }
 
-template <int STAGE, bool KC, bool MHD, bool EMIT>
-static void launch_one(dim3 grid, dim3 block, const StageMaps& maps, const Geometry& g,
-                       const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
-                       int kchunk, cudaStream_t st) {
+template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV>
+static void launch_one(dim3 grid, const StageMaps& maps, const Geometry& g, const Physics& ph,
+                       const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
     static bool configured = false;
-    constexpr size_t smem = Shape<MHD>::smem;
+    constexpr size_t smem = Shape<MHD, TYV>::smem;
     if (!configured) {
-        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
         configured = true;
     }
-    block.y = Shape<MHD>::ty / Cells<MHD, STAGE>::cpt;
-    stage_fp64<STAGE, KC, MHD, EMIT><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
+    const dim3 block(TX, TYV / Cells<MHD, STAGE, TYV>::cpt, 1);
+    stage_fp64<STAGE, KC, MHD, EMIT, TYV><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
 }
 
-template <bool MHD, bool EMIT>
+template <bool MHD, bool EMIT, int TYV>
 static void launch_stage(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                          const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
-    constexpr int TY = Shape<MHD>::ty;
-    dim3 block(TX, TY, 1);  // rows per thread set per stage in launch_one
-    dim3 grid((g.npx + TX - 1) / TX, (g.npy + TY - 1) / TY, (g.npz + kchunk - 1) / kchunk);
+    const dim3 grid((g.npx + TX - 1) / TX, (g.npy + TYV - 1) / TYV, (g.npz + kchunk - 1) / kchunk);
     const bool kc = ph.kappa_const != 0;
-    if (stage == 0) kc ? launch_one<0, true, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-                       : launch_one<0, false, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
-    else if (stage == 1) kc ? launch_one<1, true, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-                            : launch_one<1, false, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
-    else kc ? launch_one<2, true, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st)
-            : launch_one<2, false, MHD, EMIT>(grid, block, maps, g, ph, L, fs, sc, kchunk, st);
+    if (stage == 0) kc ? launch_one<0, true, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+                       : launch_one<0, false, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+    else if (stage == 1) kc ? launch_one<1, true, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+                            : launch_one<1, false, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+    else kc ? launch_one<2, true, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+            : launch_one<2, false, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+}
+
+template <bool EMIT>
+static void launch_any(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
+                       const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
+    if (!ph.lmag) launch_stage<false, EMIT, R3D_STAGE_TY>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+    else if (g.tile_rows == 6) launch_stage<true, EMIT, 6>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+    else launch_stage<true, EMIT, 8>(stage, maps, g, ph, L, fs, sc, kchunk, st);
 }
 
 cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
                               const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,
                               int kchunk, cudaStream_t st, bool emit_rhs) {
-    if (emit_rhs) {
-        if (ph.lmag) launch_stage<true, true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
-        else launch_stage<false, true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
-    } else {
-        if (ph.lmag) launch_stage<true, false>(stage, maps, g, ph, L, fs, sc, kchunk, st);
-        else launch_stage<false, false>(stage, maps, g, ph, L, fs, sc, kchunk, st);
-    }
+    if (ph.lmag && g.tile_rows != 6 && g.tile_rows != 8) return cudaErrorInvalidValue;
+    if (!ph.lmag && g.tile_rows != R3D_STAGE_TY) return cudaErrorInvalidValue;
+    if (emit_rhs) launch_any<true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+    else launch_any<false>(stage, maps, g, ph, L, fs, sc, kchunk, st);
     return cudaGetLastError();
 }
 
