@@ -307,8 +307,8 @@ def run_reference_arm(args, world, rank, pg):
         from oracle import Reference
 
         if not Reference.available():
-            print(json.dumps({**base, "impl": "reference",
-                              "unavailable": "reference CPU build oracle/_ref/libr3dref.so not present"}))
+            emit({**base, "impl": "reference",
+                  "unavailable": "reference CPU build oracle/_ref/libr3dref.so not present"})
             return 0
         ncores = os.cpu_count() or 1
         nz = 16
@@ -329,14 +329,31 @@ def run_reference_arm(args, world, rank, pg):
                "cpu_baseline": {"value": v, "unit": UNIT, "cores": ranks * threads, "kind": "reference",
                                 "sample": sample},
                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(out))
+        emit(out)
     except Exception as e:
-        print(json.dumps({**base, "unavailable": f"reference CPU run failed: {e}"}))
+        emit({**base, "unavailable": f"reference CPU run failed: {e}"})
     return 0
 
 
+_RESULT = None  # stdout as it was at start: the JSON line goes there and nowhere else
+
+
+def emit(obj):
+    """Print the one JSON result line on the original stdout."""
+    out = _RESULT if _RESULT is not None else sys.stdout
+    out.write(json.dumps(obj) + "\n")
+    out.flush()
+
+
 def main():
-    # the JSON line is the only output on stdout: NCCL's version banner stays off
+    # The JSON line must be the only output on stdout.  Libraries print there too (NCCL writes
+    # its version line at any NCCL_DEBUG level from WARN up, and INFO logs), so file descriptor 1
+    # is pointed at stderr for the whole run and the result is written to a duplicate of the
+    # original stdout.
+    global _RESULT
+    sys.stdout.flush()
+    _RESULT = os.fdopen(os.dup(1), "w")
+    os.dup2(2, 1)
     os.environ.setdefault("NCCL_DEBUG", "WARN")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -367,7 +384,7 @@ def main():
             SEED = 11
             fl = ["--tp", "2", "--tc", "0", "--xp", "10", "--yp", "10", "--zp", "0", "--hh", "1"]
         g = args.fp32_error
-        print(json.dumps(fp32_error_run(R, 0, g[:3], g[3], fl)))
+        emit(fp32_error_run(R, 0, g[:3], g[3], fl))
         return 0
     global GRID, FLAGS
     if args.grid:
@@ -491,7 +508,7 @@ def main():
                               "note": "full re-evaluations of the third stage's filtered dt limits "
                                       "(-1: slab handle, filter off)"},
                "extra": extra}
-        print(json.dumps(out))
+        emit(out)
     if pg is not None:
         pg.destroy_process_group()
     return 0

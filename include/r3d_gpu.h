@@ -139,6 +139,9 @@ int r3d_mesh_step(r3d_mesh* m, int nstages, r3d_scalars* sc);
 int r3d_mesh_run(r3d_mesh* m, int nsteps, r3d_scalars* sc);
 int r3d_mesh_download(r3d_mesh* m, r3d_host_state* st, r3d_scalars* sc);
 int r3d_mesh_destroy(r3d_mesh* m);
+/* Test hook: r3d_gpu_debug_dt_filter on every slab of the mesh; *refolds (may be NULL) receives
+ * the refolds of all slabs together. */
+int r3d_mesh_debug_dt_filter(r3d_mesh* m, double margin, int* refolds);
 
 /* FLUXES (src/fluxes.cpp:44-533; with lmag the LMAG branch of 3dmhdsub.f:2146-2650) of the
  * current device state, without changing it: out = nfields host arrays (NX*NY*NZ) receiving
@@ -160,8 +163,10 @@ int r3d_gpu_debug_tma_extra(r3d_gpu* g, unsigned int bytes);
  * fails the check that makes this exact, the limits are evaluated again over the whole state
  * (a "refold").  The dt is bit-identical either way.  Test hook: margin (NaN: unchanged) sets
  * the margin - a negative one makes every full step refold - and *refolds (may be NULL)
- * receives the number of refolds since the upload, or -1 on a slab handle, where the filter
- * keeps only its exact running bounds. */
+ * receives the number of refolds since the upload.  A z-slab handle (r3d_gpu_create_slab, the
+ * mesh) takes its thresholds from its own limits, saved before they are combined with the
+ * other slabs', and checks its own fold, so each slab's limits - and their minimum over the
+ * slabs - stay exact. */
 int r3d_gpu_debug_dt_filter(r3d_gpu* g, double margin, int* refolds);
 
 /* Bytes of device memory held by g. */

@@ -163,9 +163,12 @@ __global__ void step_begin_kernel(Physics ph, Scalars* sc) {
     const double u = order_value(sc->umax);
     sc->umach = sqrt(u);
     // thresholds of this step's filtered fold: the previous limits widened by the margin (a
-    // margin < 0 forces the re-evaluation path; thr_on == 0 leaves only the exact running bounds)
-    sc->thr_w1 = sc->thr_on ? w0 * (1.0 + sc->thr_margin) : 1e308;
-    sc->thr_um = sc->thr_on ? u * (1.0 - sc->thr_margin) : 0.0;
+    // margin < 0 forces the re-evaluation path; thr_on == 0 leaves only the exact running bounds);
+    // a slab takes its own limits, so that its check at step_end makes its own fold exact
+    const double tw = sc->thr_local ? order_value(sc->wloc[0]) : w0;
+    const double tu = sc->thr_local ? order_value(sc->uloc) : u;
+    sc->thr_w1 = sc->thr_on ? tw * (1.0 + sc->thr_margin) : 1e308;
+    sc->thr_um = sc->thr_on ? tu * (1.0 - sc->thr_margin) : 0.0;
     sc->wmin[0] = sc->wmin[1] = sc->wmin[2] = sc->wmin[3] = order_key(1e300);
     sc->umax = order_key(0.0);
 }
@@ -190,6 +193,11 @@ __global__ void step_end_kernel(Scalars* sc, int check) {
     sc->refold = refold;
 }
 
+__global__ void save_local_limits_kernel(Scalars* sc) {
+    for (int q = 0; q < 4; ++q) sc->wloc[q] = sc->wmin[q];
+    sc->uloc = sc->umax;
+}
+
 __global__ void reset_reduction_kernel(Scalars* sc) {
     sc->wmin[0] = sc->wmin[1] = sc->wmin[2] = sc->wmin[3] = order_key(1e300);
     sc->umax = order_key(0.0);
@@ -201,6 +209,10 @@ cudaError_t launch_step_begin(const Physics& ph, Scalars* sc, cudaStream_t st) {
 }
 cudaError_t launch_step_end(Scalars* sc, cudaStream_t st, int check) {
     step_end_kernel<<<1, 1, 0, st>>>(sc, check);
+    return cudaGetLastError();
+}
+cudaError_t launch_save_local_limits(Scalars* sc, cudaStream_t st) {
+    save_local_limits_kernel<<<1, 1, 0, st>>>(sc);
     return cudaGetLastError();
 }
 cudaError_t launch_reset_reduction(Scalars* sc, cudaStream_t st) {

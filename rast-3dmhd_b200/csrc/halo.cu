@@ -93,6 +93,7 @@ void halo_reduce_limits(r3d_gpu* g) {
     Range r("r3d.halo_reduce");
     Halo* h = g->halo;
     Nccl& n = nccl();
+    cuda_ok(r3dk::launch_save_local_limits(g->dsc, g->stream), "save local limits");
     nccl_ok(n.groupStart(), "ncclGroupStart");
     nccl_ok(n.allReduce(g->dsc->wmin, g->dsc->wmin, 4, ncclUint64, ncclMin, h->comm, g->stream), "ncclAllReduce(min)");
     nccl_ok(n.allReduce(&g->dsc->umax, &g->dsc->umax, 1, ncclUint64, ncclMax, h->comm, g->stream), "ncclAllReduce(max)");

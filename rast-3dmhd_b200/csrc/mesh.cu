@@ -29,6 +29,10 @@ struct r3d_mesh {
 namespace {
 
 __global__ void mesh_reduce_kernel(r3dk::Scalars** s, int n) {
+    for (int r = 0; r < n; ++r) {  // each slab's own limits, for its dt filter thresholds
+        for (int q = 0; q < 4; ++q) s[r]->wloc[q] = s[r]->wmin[q];
+        s[r]->uloc = s[r]->umax;
+    }
     unsigned long long w[4], u = s[0]->umax;
     for (int q = 0; q < 4; ++q) w[q] = s[0]->wmin[q];
     for (int r = 1; r < n; ++r) {
@@ -179,6 +183,19 @@ int r3d_mesh_download(r3d_mesh* m, r3d_host_state* st, r3d_scalars* sc) {
             if (rc != R3D_OK) throw Error(rc, r3d_last_error());
         }
     });
+}
+
+int r3d_mesh_debug_dt_filter(r3d_mesh* m, double margin, int* refolds) {
+    if (!m) return R3D_EINVAL;
+    int total = 0;
+    for (r3d_gpu* g : m->slabs) {
+        int n = 0;
+        const int rc = r3d_gpu_debug_dt_filter(g, margin, refolds ? &n : nullptr);
+        if (rc != R3D_OK) return rc;
+        total += n;
+    }
+    if (refolds) *refolds = total;
+    return R3D_OK;
 }
 
 int r3d_mesh_destroy(r3d_mesh* m) {

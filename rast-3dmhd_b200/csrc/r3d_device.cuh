@@ -77,10 +77,13 @@ struct Scalars {
     // thr_margin; step_end sets refold when the filtered minimum/maximum fails the check, and
     // the limits are then evaluated again over the whole state.
     int thr_on;
+    int thr_local;  // a slab: thresholds from its own limits (wloc, uloc), saved before they are
+                    // combined with the other slabs' (the check at step_end is then per slab)
     int refold;
     int refolds;  // number of re-evaluations since the upload (diagnostic)
     double thr_margin;
     double thr_w1, thr_um;
+    unsigned long long wloc[4], uloc;  // this slab's limit keys before the cross-slab reduction
 };
 
 // Total order on doubles as unsigned keys: key(a) < key(b) iff a < b (NaN excluded).

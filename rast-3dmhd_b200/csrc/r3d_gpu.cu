@@ -577,7 +577,6 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             g->geo.top_edge = z0 == 0 ? 1 : 0;
             g->geo.bot_edge = z0 + nloc == p->npz ? 1 : 0;
             g->geo.tile_rows = r3dk::stage_fp64_rows(p->lmag, p->npx, p->npy, nloc);
-            g->dt_filter = z0 == 0 && nloc == p->npz;
             g->geo.pitch = (d.nx + 15) / 16 * 16;
             g->geo.plane = g->geo.pitch * d.ny;
             if (g->geo.plane * d.nz >= (int64_t(1) << 31))
@@ -789,6 +788,7 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
         h.dt = sc->dt; h.timc = sc->timc; h.timt = sc->timt; h.timi = sc->timi;
         h.umach = sc->umach; h.tb = sc->tb; h.nit = sc->nit;
         h.thr_on = g->dt_filter ? 1 : 0;
+        h.thr_local = (g->z0 != 0 || g->nloc != g->p.npz) ? 1 : 0;
         h.thr_margin = g->thr_margin;
         *g->hsc = h;
         cuda_ok(cudaMemcpyAsync(g->dsc, g->hsc, sizeof(h), cudaMemcpyHostToDevice, g->stream), "upload scalars");
@@ -903,7 +903,7 @@ int r3d_gpu_debug_dt_filter(r3d_gpu* g, double margin, int* refolds) {
                     "refolds");
         }
         cuda_ok(cudaStreamSynchronize(g->stream), "dt filter");
-        if (refolds) *refolds = g->dt_filter ? g->hsc->refolds : -1;
+        if (refolds) *refolds = g->hsc->refolds;
     });
 }
 

@@ -57,9 +57,9 @@ struct r3d_gpu {
     bool own_stream = true;
     r3dg::Halo* halo = nullptr;              // ghost-plane exchange with other slabs (NCCL)
     double* fscr = nullptr;                  // r3d_gpu_fluxes scratch: X', Z', F (nfields each)
-    // threshold filter of the third stage's limits (whole-domain handles only: a slab's own
-    // limits are not the domain's, and its thresholds would come from the reduced ones)
-    bool dt_filter = false;
+    // threshold filter of the third stage's limits (on a slab: thresholds and check from the
+    // slab's own limits, Scalars::thr_local)
+    bool dt_filter = true;
     double thr_margin = 1.0 / 64.0;
     // two whole steps captured as a CUDA graph, one per state-buffer parity at capture (r3d_gpu_run
     // replays it; six stages leave the parity unchanged)

@@ -76,6 +76,8 @@ cudaError_t launch_step_begin(const Physics& ph, Scalars* sc, cudaStream_t st);
 // check: verify the filtered limits of a full step (Scalars::thr_*), request a refold if needed
 cudaError_t launch_step_end(Scalars* sc, cudaStream_t st, int check = 0);
 cudaError_t launch_reset_reduction(Scalars* sc, cudaStream_t st);
+// copy the limit keys to Scalars::wloc/uloc (a slab, before its keys are combined with others')
+cudaError_t launch_save_local_limits(Scalars* sc, cudaStream_t st);
 cudaError_t launch_totals(const Geometry& g, const Physics& ph, const FieldSet& fs, Scalars* sc,
                           cudaStream_t st);
 

@@ -123,6 +123,7 @@ def lib():
         L.r3d_mesh_run.argtypes = [vp, ip, ctypes.POINTER(Scalars)]
         L.r3d_mesh_download.argtypes = [vp, ctypes.POINTER(_HostStateC), ctypes.POINTER(Scalars)]
         L.r3d_mesh_destroy.argtypes = [vp]
+        L.r3d_mesh_debug_dt_filter.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         dpp = ctypes.POINTER(ctypes.POINTER(ctypes.c_double))
         L.r3d_gpu_adjoint_record.argtypes = [vp, ip, ip, ctypes.POINTER(Scalars)]
         L.r3d_gpu_adjoint_backward.argtypes = [vp, dpp, dpp]
@@ -450,6 +451,13 @@ class GpuMesh:
         sc = Scalars()
         _check(lib().r3d_mesh_step(self.h, nstages, ctypes.byref(sc)))
         return sc.as_dict()
+
+    def debug_dt_filter(self, margin: float = float("nan")) -> int:
+        """Test hook: the dt-filter margin of every slab (NaN: unchanged); returns the refolds
+        of all slabs since the upload."""
+        n = ctypes.c_int(0)
+        _check(lib().r3d_mesh_debug_dt_filter(self.h, margin, ctypes.byref(n)))
+        return n.value
 
     def run(self, nsteps: int) -> Dict[str, float]:
         sc = Scalars()

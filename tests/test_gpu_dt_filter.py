@@ -84,9 +84,26 @@ def test_fp32bulk_forced_refold_identical():
 
 
 @pytest.mark.gpu
-def test_slab_handle_reports_no_filter():
-    p = R.parse(["--npx", "16", "--npy", "16", "--npz", "16"])
-    with R.GpuSim(p, slab=(4, 8)) as sim:
-        assert sim.debug_dt_filter() == -1
-    with R.GpuSim(p) as sim:
-        assert sim.debug_dt_filter() == 0
+@pytest.mark.parametrize("margin", [None, -0.5])
+def test_slabs_filter_on_their_own_limits(margin):
+    """z slabs take their thresholds from their own limits and check their own folds: with
+    the default margin (rare refolds) and with a negative one (every slab refolds every step)
+    the mesh reproduces the single domain bit for bit."""
+    flags = ["--npx", "40", "--npy", "24", "--npz", "48", "--seed", "9"]
+    p = R.parse(flags)
+    ref, dts, _ = run(flags[:-2], 9, 6)
+    st = R.HostState.setup(p)
+    with R.GpuMesh(p, 3) as m:
+        if margin is not None:
+            m.debug_dt_filter(margin)
+        m.upload(st)
+        got = [m.step()["dt"] for _ in range(6)]
+        refolds = m.debug_dt_filter()
+        m.download(st)
+    assert got == dts
+    for n in FIELDS[:5]:
+        assert np.array_equal(interior(st.fields[n]), interior(ref.fields[n])), n
+    if margin is not None:
+        assert refolds == 6 * 3
+    else:
+        assert refolds <= 3
