@@ -60,6 +60,27 @@ class NumpyStep:
               "d2zzdz2", "ddz", "rkapa", "dkapa"]}
         self.L = L
         self.timi = o.scalars()["timi"]
+        # z slab held (the whole domain by default): one-sided z stencils and BCON only on the
+        # domain's faces; hooks for the multi-rank form (the reduction of the dt minimum over
+        # the slabs and the ghost-plane exchange after every stage)
+        self.top = self.bot = True
+        self.z0 = 0
+        self.reduce_min = None
+        self.exchange = None
+
+    def slab(self, z0: int, nloc: int) -> "NumpyStep":
+        """The same step on global planes z0+1 .. z0+nloc, with the neighbours' planes as
+        ghost planes (the decomposition of src/communicate.cpp over npez ranks)."""
+        import copy
+        s = copy.copy(self)
+        s.L = dict(self.L)
+        for n in ("dzzdz", "d2zzdz2", "ddz", "rkapa", "dkapa"):
+            s.L[n] = self.L[n][z0:z0 + nloc + 2].copy()
+        s.NZ = nloc + 2
+        s.z0 = z0
+        s.top = z0 == 0
+        s.bot = z0 + nloc == self.npz
+        return s
 
     # ------------------------------------------------------------------ helpers ------------
     def _box(self, kr, jr, ir):
@@ -121,16 +142,22 @@ class NumpyStep:
         I = slice(1, self.NX - 1)
         dz1, dz2 = self.L["dzzdz"][k1], self.L["dzzdz"][k2]
         if not second:
-            out[0] = (4.0 * f[k1 + 1, J, I] - f[k1 + 2, J, I]) * (self.hz * dz1)
-            out[-1] = (f[k2 - 2, J, I] - 4.0 * f[k2 - 1, J, I]) * (self.hz * dz2)
+            if self.top:
+                out[0] = (4.0 * f[k1 + 1, J, I] - f[k1 + 2, J, I]) * (self.hz * dz1)
+            if self.bot:
+                out[-1] = (f[k2 - 2, J, I] - 4.0 * f[k2 - 1, J, I]) * (self.hz * dz2)
         else:
             d21, d22 = self.L["d2zzdz2"][k1], self.L["d2zzdz2"][k2]
-            out[0] = ((-3.0 * f[k1, J, I] + 4.0 * f[k1 + 1, J, I] - f[k1 + 2, J, I]) * self.hz * d21 +
+            top = ((-3.0 * f[k1, J, I] + 4.0 * f[k1 + 1, J, I] - f[k1 + 2, J, I]) * self.hz * d21 +
                       (2.0 * f[k1, J, I] - 5.0 * f[k1 + 1, J, I] + 4.0 * f[k1 + 2, J, I] - f[k1 + 3, J, I]) *
                       self.h2z * dz1 * dz1)
-            out[-1] = ((3.0 * f[k2, J, I] - 4.0 * f[k2 - 1, J, I] + f[k2 - 2, J, I]) * self.hz * d22 +
+            if self.top:
+                out[0] = top
+            bot = ((3.0 * f[k2, J, I] - 4.0 * f[k2 - 1, J, I] + f[k2 - 2, J, I]) * self.hz * d22 +
                        (2.0 * f[k2, J, I] - 5.0 * f[k2 - 1, J, I] + 4.0 * f[k2 - 2, J, I] - f[k2 - 3, J, I]) *
                        self.h2z * dz2 * dz2)
+            if self.bot:
+                out[-1] = bot
         return out
 
     # ------------------------------------------------------------------ FLUXES -------------
@@ -298,6 +325,8 @@ class NumpyStep:
         ru, rv, rw, ro, tt = (X[n] for n in HYDRO)
         k1, k2 = 1, self.NZ - 2
         for k, d in ((k1, 1), (k2, -1)):
+            if (k == k1 and not self.top) or (k == k2 and not self.bot):
+                continue  # a neighbour's plane, not a face of the domain
             ru[k, J, I] = ro[k, J, I] * (c43 * ru[k + d, J, I] / ro[k + d, J, I] - c13 * ru[k + 2 * d, J, I] / ro[k + 2 * d, J, I])
             rv[k, J, I] = ro[k, J, I] * (c43 * rv[k + d, J, I] / ro[k + d, J, I] - c13 * rv[k + 2 * d, J, I] / ro[k + 2 * d, J, I])
             rw[k, J, I] = 0.0
@@ -358,6 +387,8 @@ class NumpyStep:
                 i = int(np.nanargmin(flat))
                 if best is None or flat[i] < best:
                     best, bq, bi = flat[i], q, i
+        if self.reduce_min is not None:  # a slab: the minimum over every slab (real runs only)
+            return self.sff * self.reduce_min(float(best) if best is not None else 1e300)
         return self.sff * wc[bq].reshape(-1)[bi]
 
     def _limits(self, X):
@@ -405,6 +436,8 @@ class NumpyStep:
             self.bcon(X)
             for n in names:
                 self.ghost_fill(X[n])
+            if self.exchange is not None:
+                self.exchange(X)
         return X, dt
 
     def run(self, X, nsteps: int):

@@ -76,3 +76,82 @@ def test_unique_id_broadcast_two_ranks():
 def test_nccl_unique_id_is_128_bytes():
     uid = R.nccl_unique_id()
     assert isinstance(uid, bytes) and len(uid) == 128
+
+
+def _slab_rank(rank, world, port, q, flags, seed, nsteps):
+    """One rank of the multi-process z-slab step on the CPU: the numpy restatement of the step on
+    this rank's slab, ghost planes swapped with the z neighbours after every stage and the dt
+    minimum all-reduced before every step - the protocol the NCCL path runs on GPUs."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import Oracle
+        from tangent_np import NumpyStep
+
+        o = Oracle(flags).init(seed)
+        full = NumpyStep(o)
+        X0 = {n: o.field(n).copy() for n in full.fields}
+        z0, nz = D.slab_of(full.npz, rank, world)
+        s = full.slab(z0, nz)
+
+        def reduce_min(x):
+            t = torch.tensor([x], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MIN)
+            return float(t.item())
+
+        def exchange(X):
+            reqs, recv = [], []
+            for n in s.fields:
+                a = X[n]
+                if rank > 0:    # my first plane up, the slab above's last plane into my plane 0
+                    reqs.append(dist.isend(torch.from_numpy(a[1].copy()), rank - 1))
+                    recv.append((n, 0, torch.empty(a[0].shape, dtype=torch.float64), rank - 1))
+                if rank < world - 1:
+                    reqs.append(dist.isend(torch.from_numpy(a[nz].copy()), rank + 1))
+                    recv.append((n, nz + 1, torch.empty(a[0].shape, dtype=torch.float64), rank + 1))
+            for n, k, t, src in recv:
+                dist.recv(t, src)
+                X[n][k] = t.numpy()
+            for r in reqs:
+                r.wait()
+
+        s.reduce_min, s.exchange = reduce_min, exchange
+        X = {n: a[z0:z0 + nz + 2].copy() for n, a in X0.items()}
+        Xs, dts = s.run(X, nsteps)
+        Xf, dtf = full.run(X0, nsteps)       # the single domain, for comparison
+        same = all(np.array_equal(Xs[n][1:-1, 1:-1, 1:-1], Xf[n][z0 + 1:z0 + nz + 1, 1:-1, 1:-1]) for n in s.fields)
+        q.put((rank, same, dts == dtf, s.top, s.bot))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("flags,world", [
+    (["--npx", "12", "--npy", "10", "--npz", "16"], 2),
+    (["--npx", "10", "--npy", "8", "--npz", "20", "--lmag", "1", "--beta", "10", "--rm", "1", "--ampb", "0.1",
+      "--bfh", "2", "--bzp", "20"], 3),
+], ids=["hydro_2ranks", "mhd_3ranks"])
+def test_multirank_slab_protocol_equals_single_domain(flags, world):
+    """gloo ranks on the CPU run the z-slab decomposition (exchange after each stage, dt
+    all-reduce per step) and reproduce the single-domain step bit for bit."""
+    import multiprocessing as mp
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_slab_rank, args=(r, world, port, q, flags, 5, 3)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    out = sorted(q.get(timeout=300) for _ in range(world))
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    assert all(o[1] for o in out), out
+    assert all(o[2] for o in out), out
+    assert out[0][3] and not out[0][4] and out[-1][4] and not out[-1][3]
