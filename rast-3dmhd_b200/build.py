@@ -55,9 +55,11 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
             extra = ["-Xptxas", "-v"] if (verbose_ptxas and s.endswith(".cu")) else []
             lang = ["-x", "cu"] if s.endswith(".cu") else ["-x", "c++"]
             fmad = ["-fmad=true"] if s in FMAD_ON else ["-fmad=false"]
-            _run([NVCC] + ARCH + COMMON + fmad + extra + lang + ["-c", src, "-o", obj])
+            omp = ["-Xcompiler", "-fopenmp"] if s in HOST_SRCS else []  # host set-up loops
+            _run([NVCC] + ARCH + COMMON + fmad + omp + extra + lang + ["-c", src, "-o", obj])
     if force or _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs + ["-cudart", "static", "-ldl"])
+        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs +
+             ["-cudart", "static", "-ldl", "-lgomp"])
     main = os.path.join(PKG, "host", "r3d_main.cpp")
     if os.path.exists(main) and (force or _stale(BIN, [main, LIB])):
         _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),

@@ -308,6 +308,7 @@ void static_profile(const r3d_params& p, std::vector<double>& T, std::vector<dou
 }
 
 void fill_ghosts(double* f, int64_t nx, int64_t ny, int64_t nz) {
+#pragma omp parallel for schedule(static)
     for (int64_t k = 0; k < nz; ++k) {
         double* pl = f + k * nx * ny;
         std::memcpy(pl, pl + (ny - 2) * nx, sizeof(double) * nx);
@@ -344,15 +345,21 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc,
     putz(st.zee, m.z.s); putz(st.dzzdz, m.z.d1); putz(st.d2zzdz2, m.z.d2); putz(st.ddz, m.z.dd);
     putz(st.rkapa, m.rkapa); putz(st.dkapa, m.dkapa);
 
-    for (double* a : {st.ru, st.rv, st.rw, st.ro, st.tt}) std::memset(a, 0, sizeof(double) * N);
-    if (p.lmag)
-        for (double* a : {st.bx, st.by, st.bz}) std::memset(a, 0, sizeof(double) * N);
+    // zero every field plane by plane over the host threads (the first touch of fresh pages
+    // is most of the set-up time on large grids)
+    for (double* a : {st.ru, st.rv, st.rw, st.ro, st.tt, st.bx, st.by, st.bz}) {
+        if (!a || ((a == st.bx || a == st.by || a == st.bz) && !p.lmag)) continue;
+#pragma omp parallel for schedule(static)
+        for (int64_t k = 0; k < NZ; ++k) std::memset(a + k * NX * NY, 0, sizeof(double) * NX * NY);
+    }
+    (void)N;
 
     std::vector<double> T, R;
     static_profile(p, T, R);
     const double tb = T[p.npz - 1], rb = R[p.npz - 1];
     auto at = [&](int64_t i, int64_t j, int64_t k) { return i + NX * (j + NY * k); };
     // columns (src/static_ic.cpp:53-89): ghost top = T(0), interior k = T(k-1), ghost bottom = tb
+#pragma omp parallel for schedule(static)
     for (int64_t k = 0; k < NZ; ++k) {
         const int64_t kg = z0 + k;
         const double tv = kg == 0 ? T[0] : (kg == NZG - 1 ? tb : T[kg - 1]);
@@ -373,6 +380,7 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc,
             const double bfac = p.ampb * std::exp(cln * (z - p.bzp) * (z - p.bzp));
             for (int64_t n = at(0, 0, k); n < at(0, 0, k + 1); ++n) st.bx[n] = bfac;
         }
+#pragma omp parallel for schedule(static)
         for (int64_t k = 0; k < NZ; ++k) {
             const int64_t kg = z0 + k;
             if (kg < 1 || kg > NZG - 2) continue;
