@@ -155,3 +155,25 @@ def test_multirank_slab_protocol_equals_single_domain(flags, world):
     assert all(o[1] for o in out), out
     assert all(o[2] for o in out), out
     assert out[0][3] and not out[0][4] and out[-1][4] and not out[-1][3]
+
+
+def test_missing_nccl_is_a_clear_error():
+    """Without an NCCL to load, the slab transport fails with a status and a message (no abort):
+    a fresh process, nothing loaded NCCL before, R3D_NCCL_LIBRARY pointing at nothing."""
+    import subprocess
+    import sys
+
+    code = (
+        "import ctypes, sys\n"
+        "sys.path.insert(0, %r)\n"
+        "import r3d_b200 as R\n"
+        "L = R.lib()\n"
+        "buf = ctypes.create_string_buffer(128)\n"
+        "rc = L.r3d_nccl_unique_id(buf, 128)\n"
+        "print(rc, R.lib().r3d_last_error().decode())\n"
+    ) % os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "rast-3dmhd_b200", "python")
+    env = dict(os.environ, R3D_NCCL_LIBRARY="/nonexistent/libnccl-missing.so")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120, env=env)
+    assert r.returncode == 0, r.stderr
+    rc, msg = r.stdout.split(" ", 1)
+    assert int(rc) != 0 and "NCCL is not available" in msg, r.stdout
