@@ -115,10 +115,12 @@ __global__ void adj_save_limits_kernel(const r3dk::Scalars* sc, AdjScalars* aux)
 
 // lambda_dt from the five dot products (fixed summation order), and the winning limit as
 // step_begin_kernel chooses it.
-__global__ void __launch_bounds__(256) adj_dt_sum_kernel(r3dk::Physics ph, const double* dots, int nblocks,
-                                                          double c0, double c1, double c2, double c3, double c4,
-                                                          AdjScalars* aux) {
-    __shared__ double red[256];
+// One block of kSumThreads: a fixed summation order (deterministic), many loads in flight.
+constexpr int kSumThreads = 1024;
+__global__ void __launch_bounds__(kSumThreads) adj_dt_sum_kernel(r3dk::Physics ph, const double* dots, int nblocks,
+                                                                  double c0, double c1, double c2, double c3,
+                                                                  double c4, AdjScalars* aux) {
+    __shared__ double red[kSumThreads];
     const double coef[kDots] = {c0, c1, c2, c3, c4};
     double s = 0.0;
     for (int d = 0; d < kDots; ++d) {
@@ -128,7 +130,7 @@ __global__ void __launch_bounds__(256) adj_dt_sum_kernel(r3dk::Physics ph, const
     }
     red[threadIdx.x] = s;
     __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
+    for (int w = kSumThreads / 2; w > 0; w >>= 1) {
         if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
         __syncthreads();
     }
@@ -394,7 +396,7 @@ void reverse_step(r3d_gpu* g, Adjoint* A) {
         cuda_ok(cudaGetLastError(), "adj_pass2");
         cur = 1 - cur;
     }
-    adj_dt_sum_kernel<<<1, 256, 0, g->stream>>>(g->ph, A->dots, A->nblocks, gam[2], gam[1], gam[0], zeta[2], zeta[1],
+    adj_dt_sum_kernel<<<1, kSumThreads, 0, g->stream>>>(g->ph, A->dots, A->nblocks, gam[2], gam[1], gam[0], zeta[2], zeta[1],
                                                A->aux);
     cuda_ok(cudaGetLastError(), "adj_dt_sum");
     AdjArgs d = base_args(g, A);
