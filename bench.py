@@ -505,8 +505,7 @@ def main():
                "gpu_launches": int(tm["total_launches"]), "clocks": clk.summary(),
                "final_dt": sc["dt"],
                "dt_refolds": {"count": refolds, "steps": args.warmup + args.steps,
-                              "note": "full re-evaluations of the third stage's filtered dt limits "
-                                      "(-1: slab handle, filter off)"},
+                              "note": "full re-evaluations of the third stage's filtered dt limits"},
                "extra": extra}
         emit(out)
     if pg is not None:
