@@ -339,8 +339,7 @@ class GpuSim:
 
     def debug_dt_filter(self, margin: float = float("nan")) -> int:
         """Test hook of the third stage's dt filter: set its relative margin (NaN: unchanged; < 0
-        forces a full re-evaluation every step) and return the re-evaluations since the upload
-        (-1 on a slab handle)."""
+        forces a full re-evaluation every step) and return the re-evaluations since the upload."""
         n = ctypes.c_int(0)
         _check(lib().r3d_gpu_debug_dt_filter(self.h, margin, ctypes.byref(n)))
         return n.value
