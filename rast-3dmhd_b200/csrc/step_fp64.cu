@@ -69,6 +69,14 @@ struct EdgeTag {
     static constexpr bool value = B;
 };
 
+// xp - 2.0 * x0 + xm in the reference's rounding, rn(rn(xp - rn(2 * x0)) + xm), with one FP64
+// operation fewer: 2 * x0 is exact (a power-of-two scaling, subnormals included), so
+// rn(xp - rn(2 * x0)) == rn(xp - 2 * x0) == fma(-2, x0, xp) for every x0 whose double does not
+// overflow (|x0| <= DBL_MAX / 2), zero signs and infinities included.
+__device__ __forceinline__ double d2sum(double xp, double x0, double xm) {
+    return __fma_rn(-2.0, x0, xp) + xm;
+}
+
 template <bool MHD, int TYV>
 struct Shape {
     static constexpr int ty = TYV;  // tile rows
@@ -331,28 +339,28 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
                 // ---- thermal conduction, src/fluxes.cpp:246-276 ----
                 const double td = ph.tdiff;
                 if (KC) {  // rkapa == 1, dkapa == 0: x*1 == x, ft + (+-0) == ft
-                    ft += ((Txp - Txm) * hx * d2x + (Txp - 2.0 * T0 + Txm) * h2x * dx1 * dx1) * ri * td;
-                    ft += ((Typ - Tym) * tmpy1 + (Typ - 2.0 * T0 + Tym) * tmpy2) * ri * td;
-                    ft += ((Tzp - Tzm) * tmpz1 + (Tzp - 2.0 * T0 + Tzm) * tmpz2) * ri * td;
+                    ft += ((Txp - Txm) * hx * d2x + d2sum(Txp, T0, Txm) * h2x * dx1 * dx1) * ri * td;
+                    ft += ((Typ - Tym) * tmpy1 + d2sum(Typ, T0, Tym) * tmpy2) * ri * td;
+                    ft += ((Tzp - Tzm) * tmpz1 + d2sum(Tzp, T0, Tzm) * tmpz2) * ri * td;
                 } else {
                     const double rk = L.rkapa[k], dk = L.dkapa[k];
-                    ft += ((Txp - Txm) * hx * d2x + (Txp - 2.0 * T0 + Txm) * h2x * dx1 * dx1) * ri * td * rk;
-                    ft += ((Typ - Tym) * tmpy1 + (Typ - 2.0 * T0 + Tym) * tmpy2) * ri * td * rk;
-                    ft += ((Tzp - Tzm) * tmpz1 + (Tzp - 2.0 * T0 + Tzm) * tmpz2) * ri * td * rk;
+                    ft += ((Txp - Txm) * hx * d2x + d2sum(Txp, T0, Txm) * h2x * dx1 * dx1) * ri * td * rk;
+                    ft += ((Typ - Tym) * tmpy1 + d2sum(Typ, T0, Tym) * tmpy2) * ri * td * rk;
+                    ft += ((Tzp - Tzm) * tmpz1 + d2sum(Tzp, T0, Tzm) * tmpz2) * ri * td * rk;
                     ft += (Tzp - Tzm) * hz * dzk * ri * td * dk;
                 }
 
                 // ---- viscous momentum, src/fluxes.cpp:281-320 ----
                 const double ore = ph.ore, c43 = ph.c43;
-                fu += ore * (c43 * ((Uxp - Uxm) * hx * d2x + (Uxp - 2.0 * U0 + Uxm) * h2x * dx1 * dx1) +
-                             (Uyp - Uym) * tmpy1 + (Uyp - 2.0 * U0 + Uym) * tmpy2 +
-                             (Uzp - Uzm) * tmpz1 + (Uzp - 2.0 * U0 + Uzm) * tmpz2);
-                fv += ore * (((Vxp - Vxm) * hx * d2x + (Vxp - 2.0 * V0 + Vxm) * h2x * dx1 * dx1) +
-                             c43 * ((Vyp - Vym) * tmpy1 + (Vyp - 2.0 * V0 + Vym) * tmpy2) +
-                             (Vzp - Vzm) * tmpz1 + (Vzp - 2.0 * V0 + Vzm) * tmpz2);
-                fw += ore * (((Wxp - Wxm) * hx * d2x + (Wxp - 2.0 * W0 + Wxm) * h2x * dx1 * dx1) +
-                             (Wyp - Wym) * tmpy1 + (Wyp - 2.0 * W0 + Wym) * tmpy2 +
-                             c43 * ((Wzp - Wzm) * tmpz1 + (Wzp - 2.0 * W0 + Wzm) * tmpz2));
+                fu += ore * (c43 * ((Uxp - Uxm) * hx * d2x + d2sum(Uxp, U0, Uxm) * h2x * dx1 * dx1) +
+                             (Uyp - Uym) * tmpy1 + d2sum(Uyp, U0, Uym) * tmpy2 +
+                             (Uzp - Uzm) * tmpz1 + d2sum(Uzp, U0, Uzm) * tmpz2);
+                fv += ore * (((Vxp - Vxm) * hx * d2x + d2sum(Vxp, V0, Vxm) * h2x * dx1 * dx1) +
+                             c43 * ((Vyp - Vym) * tmpy1 + d2sum(Vyp, V0, Vym) * tmpy2) +
+                             (Vzp - Vzm) * tmpz1 + d2sum(Vzp, V0, Vzm) * tmpz2);
+                fw += ore * (((Wxp - Wxm) * hx * d2x + d2sum(Wxp, W0, Wxm) * h2x * dx1 * dx1) +
+                             (Wyp - Wym) * tmpy1 + d2sum(Wyp, W0, Wym) * tmpy2 +
+                             c43 * ((Wzp - Wzm) * tmpz1 + d2sum(Wzp, W0, Wzm) * tmpz2));
 
                 // ---- viscous heating, p dV and cross terms, src/fluxes.cpp:327-514 ----
                 const double th = ph.theat, th43 = ph.theat43, t13 = ph.t13, ocv = ph.ocv;
@@ -438,12 +446,12 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
                 b1 = b1 - U0 * bxx - V0 * bxy;             // 1230
                 b2f = b2f - U0 * byx;                      // 1240
                 b3 = b3 - U0 * bzx;                        // 1250
-                const double d2bxx = (BXxp - BXxm) * hx * d2x + (BXxp - 2.0 * BX0 + BXxm) * h2x * dx1 * dx1;  // 1260
-                const double d2byx = (BYxp - BYxm) * hx * d2x + (BYxp - 2.0 * BY0 + BYxm) * h2x * dx1 * dx1;  // 1265
-                const double d2bxy = (BXyp - BXym) * hy * d2y + (BXyp - 2.0 * BX0 + BXym) * h2y * dyj * dyj;  // 1270
+                const double d2bxx = (BXxp - BXxm) * hx * d2x + d2sum(BXxp, BX0, BXxm) * h2x * dx1 * dx1;  // 1260
+                const double d2byx = (BYxp - BYxm) * hx * d2x + d2sum(BYxp, BY0, BYxm) * h2x * dx1 * dx1;  // 1265
+                const double d2bxy = (BXyp - BXym) * hy * d2y + d2sum(BXyp, BX0, BXym) * h2y * dyj * dyj;  // 1270
                 b1 = b1 + orm * (d2bxx + d2bxy);           // 1280
                 b2f = b2f + orm * d2byx;                   // 1290
-                const double d2bzx = (BZxp - BZxm) * hx * d2x + (BZxp - 2.0 * BZ0 + BZxm) * h2x * dx1 * dx1;  // 1300
+                const double d2bzx = (BZxp - BZxm) * hx * d2x + d2sum(BZxp, BZ0, BZxm) * h2x * dx1 * dx1;  // 1300
                 b3 = b3 + orm * d2bzx;                     // 1310
                 const double bxz = (BXzp - BXzm) * hz * dzk;   // 1320
                 const double byy = (BYyp - BYym) * hy * dyj;   // 1330
@@ -468,10 +476,10 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
                     d2byz = (3.0 * BY0 - 4.0 * BYzm + by2) * hz * d2z +
                             (2.0 * BY0 - 5.0 * BYzm + 4.0 * by2 - by3) * h2z * dzk * dzk;
                 } else {  // 1390, 1510
-                    d2bxz = (BXzp - BXzm) * hz * d2z + (BXzp - 2.0 * BX0 + BXzm) * h2z * dzk * dzk;
-                    d2byz = (BYzp - BYzm) * hz * d2z + (BYzp - 2.0 * BY0 + BYzm) * h2z * dzk * dzk;
+                    d2bxz = (BXzp - BXzm) * hz * d2z + d2sum(BXzp, BX0, BXzm) * h2z * dzk * dzk;
+                    d2byz = (BYzp - BYzm) * hz * d2z + d2sum(BYzp, BY0, BYzm) * h2z * dzk * dzk;
                 }
-                const double d2byy = (BYyp - BYym) * hy * d2y + (BYyp - 2.0 * BY0 + BYym) * h2y * dyj * dyj;  // 1400
+                const double d2byy = (BYyp - BYym) * hy * d2y + d2sum(BYyp, BY0, BYym) * h2y * dyj * dyj;  // 1400
                 b1 = b1 + orm * d2bxz;                     // 1410
                 b2f = b2f + orm * d2byy;                   // 1420
                 const double byz = (BYzp - BYzm) * hz * dzk;   // 1430
@@ -482,12 +490,12 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
                 ft = ft + (byz * byz + bzy * bzy - 2.0 * byz * bzy) * ri * tmag;  // 1480
                 b2f = b2f - W0 * byz;                      // 1490
                 b3 = b3 - V0 * bzy;                        // 1500
-                const double d2bzy = (BZyp - BZym) * hy * d2y + (BZyp - 2.0 * BZ0 + BZym) * h2y * dyj * dyj;  // 1520
+                const double d2bzy = (BZyp - BZym) * hy * d2y + d2sum(BZyp, BZ0, BZym) * h2y * dyj * dyj;  // 1520
                 b2f = b2f + orm * d2byz;                   // 1530
                 b3 = b3 + orm * d2bzy;                     // 1540
                 const double bzz = (BZzp - BZzm) * hz * dzk;   // 1550
                 b3 = b3 - W0 * bzz;                        // 1560
-                const double d2bzz = (BZzp - BZzm) * hz * d2z + (BZzp - 2.0 * BZ0 + BZzm) * h2z * dzk * dzk;  // 1570
+                const double d2bzz = (BZzp - BZzm) * hz * d2z + d2sum(BZzp, BZ0, BZzm) * h2z * dzk * dzk;  // 1570
                 b3 = b3 + orm * d2bzz;                     // 1580
                 if (EDGE) {  // the hydro fluxes there are rewritten by BCON: keep them finite
                     fu = fv = fw = ft = 0.0;
