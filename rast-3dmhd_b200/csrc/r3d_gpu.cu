@@ -14,8 +14,12 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -115,6 +119,48 @@ __global__ void from_fp32_kernel(double* out, const float* in, int64_t pitch, in
         const int64_t i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
         out[c] = (bg ? bg[k] : 0.0) + (double)in[k * plane + j * pitch + i];
     }
+}
+
+// Estimated length of one stage launch over `tiles` column tiles x z-chunks of depth k, in
+// plane loads: list scheduling of the CTAs in launch order (the chunk is the slowest block
+// index, so the last chunk's CTAs run last) onto `slots` resident CTA slots, each CTA costing
+// its planes plus the two halo planes.
+double launch_estimate(int64_t tiles, int nloc, int k, int64_t slots) {
+    std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+    for (int64_t s = 0; s < slots; ++s) free_at.push(0.0);
+    double end = 0.0;
+    for (int z0 = 0; z0 < nloc; z0 += k) {
+        const double cost = std::min(k, nloc - z0) + 2;
+        for (int64_t t = 0; t < tiles; ++t) {
+            const double e = free_at.top() + cost;
+            free_at.pop();
+            free_at.push(e);
+            end = std::max(end, e);
+        }
+    }
+    return end;
+}
+
+// Chunk depth of a multi-wave launch.  When the depth d divides the planes, the partial last
+// wave is full-depth CTAs and leaves most SMs idle for a whole CTA time; a slightly shallower
+// depth (at most one chunk more) with a short last chunk fills that tail.  Candidates d down to
+// 3d/4; d is kept unless the estimate improves by 0.5%, and the deepest candidate within 0.5%
+// of the best is taken (fewer halo planes).  504x504x512 FP64 on B200: 64 -> 62 planes; depths
+// 56 and 63 there measured 15.84-15.90 ms per step against 15.98-16.25 ms at 64.
+int plan_chunk_depth(int64_t tiles, int nloc, int d, int64_t slots) {
+    const int n0 = (nloc + d - 1) / d;
+    const double base = launch_estimate(tiles, nloc, d, slots);
+    std::vector<std::pair<int, double>> cand;
+    for (int k = d; k >= (3 * d + 3) / 4 && k >= 1; --k) {
+        if ((nloc + k - 1) / k > n0 + 1) break;
+        cand.emplace_back(k, launch_estimate(tiles, nloc, k, slots));
+    }
+    double best = base;
+    for (const auto& c : cand) best = std::min(best, c.second);
+    if (best > base * 0.995) return d;
+    for (const auto& c : cand)
+        if (c.second <= best * 1.005) return c.first;
+    return d;
 }
 
 }  // namespace
@@ -650,9 +696,6 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             b.bottom_mode = p->izcon;
             b.hh = p->hh; b.theta = p->theta; b.tp = p->tp; b.tpr = p->tp;
             b.half_nx = (int)(d.nx / 2);
-            #ifdef R3D_KCHUNK
-            g->kchunk = R3D_KCHUNK;
-#else
             g->kchunk = nloc >= 512 ? 64 : (nloc >= 256 ? 32 : 16);
             // column tiles of the stage kernel (32 x rows) and its resident CTAs per SM
             unsigned tbx = 0, tby = 0;
@@ -660,7 +703,12 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             else r3dk::stage_fp64_box(g->geo.tile_rows, &tbx, &tby);
             const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + (int)tby - 3) / ((int)tby - 2));
             const int64_t slots = 148 * ((g->fp32 ? 3 : 2) - (p->lmag && tby == 10 ? 1 : 0));
-            if (p->lmag) {
+            if (p->lmag && tby == 8) {
+                // 32x6 MHD tiles, two CTAs per SM: 12-plane chunks.  Measured on B200 against the
+                // earlier 16/32-plane choice: 126x126x256 0.962 -> 0.922 ms per step, 252x252x256
+                // 3.24 -> 3.14-3.17 ms for any depth in 13..24 (10..13 all within 0.6%).
+                g->kchunk = 12;
+            } else if (p->lmag) {
                 // few, heavy CTAs: prefer enough z-chunks for >= 4 full waves
                 while (g->kchunk > 16 && tiles * ((nloc + g->kchunk - 1) / g->kchunk) < 4 * slots) g->kchunk /= 2;
             }
@@ -674,9 +722,15 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
                     for (int k = g->kchunk / 2; k >= 4; k /= 2)
                         if (cost(k) < cost(best)) best = k;
                     g->kchunk = best;
+                } else if (!p->lmag && ctas(g->kchunk) <= 64 * slots) {
+                    g->kchunk = plan_chunk_depth(tiles, nloc, g->kchunk, slots);
                 }
             }
-#endif
+            // R3D_KCHUNK=<planes> overrides the z-chunk depth of the stage kernels (tuning)
+            if (const char* e = getenv("R3D_KCHUNK")) {
+                const int v = atoi(e);
+                if (v >= 1) g->kchunk = v;
+            }
             cuda_ok(cudaStreamSynchronize(g->stream), "create");
     } catch (...) {
         destroy_handle(g);
