@@ -169,6 +169,17 @@ int r3d_gpu_debug_tma_extra(r3d_gpu* g, unsigned int bytes);
  * slabs - stay exact. */
 int r3d_gpu_debug_dt_filter(r3d_gpu* g, double margin, int* refolds);
 
+/* Launch plan of the stage kernels for a handle created with *p over nloc local z planes (0:
+ * the whole npz, as r3d_gpu_create): *kchunk receives the z planes each CTA marches through,
+ * *tile_rows the rows of its 32-column tile.  Host-only, no device needed; R3D_KCHUNK=<planes>
+ * in the environment overrides the depth, as it does for a handle.  The depth starts at 64
+ * planes (npz >= 512), 32 (>= 256) or 16; MHD with 32x6 tiles takes 12; a launch that does not
+ * fill the GPU once takes the depth (down to 4) minimising waves x planes per chunk; a hydro
+ * launch of up to 64 waves takes a slightly shallower depth (at most one chunk more) when a
+ * list-scheduling estimate of the launch, whose last chunk's CTAs run last, finds it 0.5%
+ * shorter. */
+int r3d_gpu_plan(const r3d_params* p, int nloc, int* kchunk, int* tile_rows);
+
 /* Bytes of device memory held by g. */
 int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes);
 /* The CUDA stream (cudaStream_t) every kernel of g is launched on. */

@@ -163,6 +163,48 @@ int plan_chunk_depth(int64_t tiles, int nloc, int d, int64_t slots) {
     return d;
 }
 
+// z-chunk depth (planes per CTA) of the stage kernels of a handle over nloc local planes, given
+// its precision and FP64 column-tile rows; R3D_KCHUNK=<planes> in the environment overrides it.
+int stage_chunk_depth(const r3d_params& pin, bool fp32, int tile_rows, int nloc) {
+    const r3d_params* p = &pin;
+    int depth = nloc >= 512 ? 64 : (nloc >= 256 ? 32 : 16);
+    // column tiles of the stage kernel (32 x rows) and its resident CTAs per SM
+    unsigned tbx = 0, tby = 0;
+    if (fp32) r3dk::stage_fp32_box(&tbx, &tby);
+    else r3dk::stage_fp64_box(tile_rows, &tbx, &tby);
+    const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + (int)tby - 3) / ((int)tby - 2));
+    const int64_t slots = 148 * ((fp32 ? 3 : 2) - (p->lmag && tby == 10 ? 1 : 0));
+    if (p->lmag && tby == 8) {
+        // 32x6 MHD tiles, two CTAs per SM: 12-plane chunks.  Measured on B200 against the
+        // earlier 16/32-plane choice: 126x126x256 0.962 -> 0.922 ms per step, 252x252x256
+        // 3.24 -> 3.14-3.17 ms for any depth in 13..24 (10..13 all within 0.6%).
+        depth = 12;
+    } else if (p->lmag) {
+        // few, heavy CTAs: prefer enough z-chunks for >= 4 full waves
+        while (depth > 16 && tiles * ((nloc + depth - 1) / depth) < 4 * slots) depth /= 2;
+    }
+    {
+        // small grids, whose launch does not fill the GPU once: the chunk depth (down to 4)
+        // that minimises waves x (planes loaded per chunk)
+        auto ctas = [&](int k) { return tiles * ((nloc + k - 1) / k); };
+        auto cost = [&](int k) { return (ctas(k) + slots - 1) / slots * (k + 2); };
+        if (ctas(depth) < slots) {
+            int best = depth;
+            for (int k = depth / 2; k >= 4; k /= 2)
+                if (cost(k) < cost(best)) best = k;
+            depth = best;
+        } else if (!p->lmag && ctas(depth) <= 64 * slots) {
+            depth = plan_chunk_depth(tiles, nloc, depth, slots);
+        }
+    }
+    // R3D_KCHUNK=<planes> overrides the z-chunk depth of the stage kernels (tuning)
+    if (const char* e = getenv("R3D_KCHUNK")) {
+        const int v = atoi(e);
+        if (v >= 1) depth = v;
+    }
+    return depth;
+}
+
 }  // namespace
 
 namespace r3dk {
@@ -696,41 +738,7 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             b.bottom_mode = p->izcon;
             b.hh = p->hh; b.theta = p->theta; b.tp = p->tp; b.tpr = p->tp;
             b.half_nx = (int)(d.nx / 2);
-            g->kchunk = nloc >= 512 ? 64 : (nloc >= 256 ? 32 : 16);
-            // column tiles of the stage kernel (32 x rows) and its resident CTAs per SM
-            unsigned tbx = 0, tby = 0;
-            if (g->fp32) r3dk::stage_fp32_box(&tbx, &tby);
-            else r3dk::stage_fp64_box(g->geo.tile_rows, &tbx, &tby);
-            const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + (int)tby - 3) / ((int)tby - 2));
-            const int64_t slots = 148 * ((g->fp32 ? 3 : 2) - (p->lmag && tby == 10 ? 1 : 0));
-            if (p->lmag && tby == 8) {
-                // 32x6 MHD tiles, two CTAs per SM: 12-plane chunks.  Measured on B200 against the
-                // earlier 16/32-plane choice: 126x126x256 0.962 -> 0.922 ms per step, 252x252x256
-                // 3.24 -> 3.14-3.17 ms for any depth in 13..24 (10..13 all within 0.6%).
-                g->kchunk = 12;
-            } else if (p->lmag) {
-                // few, heavy CTAs: prefer enough z-chunks for >= 4 full waves
-                while (g->kchunk > 16 && tiles * ((nloc + g->kchunk - 1) / g->kchunk) < 4 * slots) g->kchunk /= 2;
-            }
-            {
-                // small grids, whose launch does not fill the GPU once: the chunk depth (down to 4)
-                // that minimises waves x (planes loaded per chunk)
-                auto ctas = [&](int k) { return tiles * ((nloc + k - 1) / k); };
-                auto cost = [&](int k) { return (ctas(k) + slots - 1) / slots * (k + 2); };
-                if (ctas(g->kchunk) < slots) {
-                    int best = g->kchunk;
-                    for (int k = g->kchunk / 2; k >= 4; k /= 2)
-                        if (cost(k) < cost(best)) best = k;
-                    g->kchunk = best;
-                } else if (!p->lmag && ctas(g->kchunk) <= 64 * slots) {
-                    g->kchunk = plan_chunk_depth(tiles, nloc, g->kchunk, slots);
-                }
-            }
-            // R3D_KCHUNK=<planes> overrides the z-chunk depth of the stage kernels (tuning)
-            if (const char* e = getenv("R3D_KCHUNK")) {
-                const int v = atoi(e);
-                if (v >= 1) g->kchunk = v;
-            }
+            g->kchunk = stage_chunk_depth(*p, g->fp32, g->geo.tile_rows, nloc);
             cuda_ok(cudaStreamSynchronize(g->stream), "create");
     } catch (...) {
         destroy_handle(g);
@@ -968,6 +976,22 @@ int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes) {
 }
 
 void* r3d_gpu_stream(r3d_gpu* g) { return g ? (void*)g->stream : nullptr; }
+
+int r3d_gpu_plan(const r3d_params* p, int nloc, int* kchunk, int* tile_rows) {
+    return guarded([&] {
+        if (!p || !kchunk || !tile_rows) throw std::invalid_argument("r3d_gpu_plan: null argument");
+        check_params(*p);
+        const int n = nloc > 0 ? nloc : p->npz;
+        if (n < 4 || n > p->npz) throw std::invalid_argument("r3d_gpu_plan: nloc must lie in [4, npz]");
+        const bool fp32 = p->precision == R3D_PREC_FP32BULK;
+        const int rows = r3dk::stage_fp64_rows(p->lmag, p->npx, p->npy, n);
+        unsigned bx = 0, by = 0;
+        if (fp32) r3dk::stage_fp32_box(&bx, &by);
+        else r3dk::stage_fp64_box(rows, &bx, &by);
+        *tile_rows = (int)by - 2;
+        *kchunk = stage_chunk_depth(*p, fp32, rows, n);
+    });
+}
 
 int r3d_gpu_step(r3d_gpu* g, int nstages, r3d_scalars* sc) {
     return guarded([&] {

@@ -101,6 +101,7 @@ def lib():
         L.r3d_gpu_download.argtypes = [vp, ctypes.POINTER(_HostStateC), ctypes.POINTER(Scalars)]
         L.r3d_gpu_destroy.argtypes = [vp]
         L.r3d_gpu_memory.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.r3d_gpu_plan.argtypes = [ctypes.POINTER(Params), ip, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.r3d_gpu_stream.argtypes = [vp]
         L.r3d_gpu_stream.restype = vp
         L.r3d_gpu_step.argtypes = [vp, ip, ctypes.POINTER(Scalars)]
@@ -168,6 +169,13 @@ def dims(p: Params):
     n = [ctypes.c_int64() for _ in range(3)]
     _check(lib().r3d_dims(ctypes.byref(p), *[ctypes.byref(x) for x in n]))
     return tuple(int(x.value) for x in n)
+
+
+def plan(p: Params, nloc: int = 0):
+    """(z planes per CTA, tile rows) of the stage kernels for a handle over nloc planes (0: npz)."""
+    k, r = ctypes.c_int(), ctypes.c_int()
+    _check(lib().r3d_gpu_plan(ctypes.byref(p), nloc, ctypes.byref(k), ctypes.byref(r)))
+    return k.value, r.value
 
 
 def static_profile(p: Params):

@@ -1,0 +1,68 @@
+"""Launch plan of the stage kernels (r3d_gpu_plan, the same function a handle uses at create):
+z planes per CTA and column-tile rows, on the host without a GPU."""
+import pytest
+
+import r3d_b200 as R
+
+MAG = ["--lmag", "1", "--beta", "10", "--rm", "1", "--ampb", "0.1", "--bfh", "2", "--bzp", "20"]
+
+
+def grid(npx, npy, npz, *extra):
+    return ["--npx", str(npx), "--npy", str(npy), "--npz", str(npz), *extra]
+
+
+@pytest.mark.parametrize("flags,want", [
+    (grid(504, 504, 512), (62, 8)),                             # short last chunk (8 x 62 + 16)
+    (grid(504, 504, 512, "--precision", "fp32bulk"), (62, 8)),
+    (grid(504, 504, 2048), (64, 8)),                            # > 64 waves: the tail is negligible
+    (grid(504, 504, 64), (16, 8)),
+    (grid(32, 32, 64), (4, 8)),                                 # one partial wave: waves x planes
+    (grid(126, 126, 256, *MAG), (12, 6)),                       # 32x6 MHD tiles, two CTAs per SM
+    (grid(252, 252, 256, *MAG), (12, 6)),
+    (grid(64, 64, 128, *MAG), (16, 8)),                         # too few tiles for 32x6
+], ids=["fp64_504x504x512", "fp32_504x504x512", "fp64_504x504x2048", "fp64_504x504x64", "fp64_32x32x64",
+        "mhd_126x126x256", "mhd_252x252x256", "mhd_64x64x128"])
+def test_plan_of_the_measured_grids(flags, want, monkeypatch):
+    monkeypatch.delenv("R3D_KCHUNK", raising=False)
+    assert R.plan(R.parse(flags)) == want
+
+
+def _default_depth(nloc):
+    return 64 if nloc >= 512 else (32 if nloc >= 256 else 16)
+
+
+@pytest.mark.parametrize("npx,npy", [(504, 504), (252, 252), (96, 64), (1000, 200), (33, 17)])
+@pytest.mark.parametrize("npz", [16, 40, 100, 256, 300, 512, 777, 1024])
+def test_hydro_depth_bounds(npx, npy, npz, monkeypatch):
+    """A hydro depth never exceeds the default; a multi-wave launch adds at most one chunk and
+    stays within 3/4 of the default; a single-wave launch takes a power-of-two fraction."""
+    monkeypatch.delenv("R3D_KCHUNK", raising=False)
+    k, rows = R.plan(R.parse(grid(npx, npy, npz)))
+    d = _default_depth(npz)
+    assert rows == 8 and 1 <= k <= d
+    tiles = -(-npx // 32) * -(-npy // 8)
+    if tiles * -(-npz // d) >= 2 * 148:
+        assert k >= (3 * d + 3) // 4
+        assert -(-npz // k) <= -(-npz // d) + 1
+    else:
+        assert d % k == 0 and k >= 4
+
+
+def test_slab_plan_and_errors(monkeypatch):
+    monkeypatch.delenv("R3D_KCHUNK", raising=False)
+    p = R.parse(grid(504, 504, 512))
+    assert R.plan(p, 512) == R.plan(p)
+    k, _ = R.plan(p, 171)                  # one of three z slabs
+    assert 1 <= k <= 16
+    for bad in (3, 513):
+        with pytest.raises(R.R3dError) as e:
+            R.plan(p, bad)
+        assert e.value.code == R.R3D_EINVAL
+
+
+def test_environment_overrides_depth(monkeypatch):
+    p = R.parse(grid(504, 504, 512))
+    monkeypatch.setenv("R3D_KCHUNK", "40")
+    assert R.plan(p) == (40, 8)
+    monkeypatch.setenv("R3D_KCHUNK", "0")  # ignored
+    assert R.plan(p) == (62, 8)
