@@ -8,8 +8,8 @@
 //  * the state is double-buffered (X_a -> X_b) plus one accumulator Z per field, 15 arrays for
 //    hydro instead of the reference's 28 (F, UU.., WW1..3 and the rho snapshot are never
 //    stored);
-//  * dt, umach, nit, timc, timt live on the device; a step is 8 kernel launches with no host
-//    round trip (the reference copies three full arrays to the host per step for dt,
+//  * dt, umach, nit, timc, timt live on the device; a step is 9 kernel launches (step_begin,
+//    3 x (stage, BCON), step_end, the conditional dt_full) with no host round trip (the reference copies three full arrays to the host per step for dt,
 //    src/gpu.cpp:790-823).
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -165,21 +165,20 @@ int plan_chunk_depth(int64_t tiles, int nloc, int d, int64_t slots) {
 
 // z-chunk depth (planes per CTA) of the stage kernels of a handle over nloc local planes, given
 // its precision and FP64 column-tile rows; R3D_KCHUNK=<planes> in the environment overrides it.
-int stage_chunk_depth(const r3d_params& pin, bool fp32, int tile_rows, int nloc) {
-    const r3d_params* p = &pin;
+int stage_chunk_depth(const r3d_params& p, bool fp32, int tile_rows, int nloc) {
     int depth = nloc >= 512 ? 64 : (nloc >= 256 ? 32 : 16);
     // column tiles of the stage kernel (32 x rows) and its resident CTAs per SM
     unsigned tbx = 0, tby = 0;
     if (fp32) r3dk::stage_fp32_box(&tbx, &tby);
     else r3dk::stage_fp64_box(tile_rows, &tbx, &tby);
-    const int64_t tiles = (int64_t)((p->npx + 31) / 32) * ((p->npy + (int)tby - 3) / ((int)tby - 2));
-    const int64_t slots = 148 * ((fp32 ? 3 : 2) - (p->lmag && tby == 10 ? 1 : 0));
-    if (p->lmag && tby == 8) {
+    const int64_t tiles = (int64_t)((p.npx + 31) / 32) * ((p.npy + (int)tby - 3) / ((int)tby - 2));
+    const int64_t slots = 148 * ((fp32 ? 3 : 2) - (p.lmag && tby == 10 ? 1 : 0));
+    if (p.lmag && tby == 8) {
         // 32x6 MHD tiles, two CTAs per SM: 12-plane chunks.  Measured on B200 against the
         // earlier 16/32-plane choice: 126x126x256 0.962 -> 0.922 ms per step, 252x252x256
         // 3.24 -> 3.14-3.17 ms for any depth in 13..24 (10..13 all within 0.6%).
         depth = 12;
-    } else if (p->lmag) {
+    } else if (p.lmag) {
         // few, heavy CTAs: prefer enough z-chunks for >= 4 full waves
         while (depth > 16 && tiles * ((nloc + depth - 1) / depth) < 4 * slots) depth /= 2;
     }
@@ -193,7 +192,7 @@ int stage_chunk_depth(const r3d_params& pin, bool fp32, int tile_rows, int nloc)
             for (int k = depth / 2; k >= 4; k /= 2)
                 if (cost(k) < cost(best)) best = k;
             depth = best;
-        } else if (!p->lmag && ctas(depth) <= 64 * slots) {
+        } else if (!p.lmag && ctas(depth) <= 64 * slots) {
             depth = plan_chunk_depth(tiles, nloc, depth, slots);
         }
     }
