@@ -13,8 +13,8 @@
 // and the B fluxes WW1..WW3) receives its terms in the reference's order, so with FMA
 // contraction off (-fmad=false) the result is bit-identical.
 //
-// Pipeline: a CTA owns a 32 x TY column tile (TY = 8 hydro, 6 MHD) and marches down a chunk of
-// z planes.  Thread 0
+// Pipeline: a CTA owns a 32 x TY column tile (TY = 8 hydro; 6, or 8 on small grids, with MHD)
+// and marches down a chunk of z planes (depth chosen per handle on the host).  Thread 0
 // streams the state fields of each plane, with a one-cell x/y halo, into a 4-slot ring by TMA
 // (one (34, TY+2, 1) box per field, completion on a per-slot mbarrier), two planes ahead of
 // the plane being computed.  Each loaded cell is then turned once into 1/rho, u, v, w and
