@@ -170,15 +170,17 @@ int r3d_gpu_debug_tma_extra(r3d_gpu* g, unsigned int bytes);
 int r3d_gpu_debug_dt_filter(r3d_gpu* g, double margin, int* refolds);
 
 /* Launch plan of the stage kernels for a handle created with *p over nloc local z planes (0:
- * the whole npz, as r3d_gpu_create): *kchunk receives the z planes each CTA marches through,
- * *tile_rows the rows of its 32-column tile.  Host-only, no device needed; R3D_KCHUNK=<planes>
- * in the environment overrides the depth, as it does for a handle.  The depth starts at 64
+ * the whole npz, as r3d_gpu_create) on a device with num_sms multiprocessors: *kchunk receives
+ * the z planes each CTA marches through, *tile_rows the rows of its 32-column tile.  With
+ * num_sms > 0 this is host-only (no device needed); num_sms <= 0 reads the SM count of device
+ * p->gpu_id, as a handle does at create.  R3D_KCHUNK=<planes> in the environment (a whole
+ * number, clamped to [1, nloc]) overrides the depth, as it does for a handle.  The depth starts at 64
  * planes (npz >= 512), 32 (>= 256) or 16; MHD with 32x6 tiles takes 12; a launch that does not
  * fill the GPU once takes the depth (down to 4) minimising waves x planes per chunk; a hydro
  * launch of up to 64 waves takes a slightly shallower depth (at most one chunk more) when a
  * list-scheduling estimate of the launch, whose last chunk's CTAs run last, finds it 0.5%
  * shorter. */
-int r3d_gpu_plan(const r3d_params* p, int nloc, int* kchunk, int* tile_rows);
+int r3d_gpu_plan(const r3d_params* p, int nloc, int num_sms, int* kchunk, int* tile_rows);
 
 /* Bytes of device memory held by g. */
 int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes);
@@ -238,9 +240,10 @@ int r3d_gpu_adjoint_memory(const r3d_gpu* g, int64_t* bytes);
  *   lines:  4 device pointers ddx[npx+2], ddy[npy+2], ddz[npz+2], rkapa[npz+2];
  *   out:    device pointer to 2 doubles, receives dt and umach;
  *   stream: cudaStream_t to launch on (NULL = legacy default stream); runs on device p->gpu_id.
- * Limit: ceil(npx/32)*ceil(npy/8) <= 65536 column tiles, else R3D_EINVAL.  Calls share the
- * array, so calls that overlap on the GPU race; the first call on a device looks up the
- * array's address and should come before any stream capture.  Allocates no device memory. */
+ * Limit: ceil(npx/32)*ceil(npy/8) <= 65536 column tiles and ceil(npy/8) <= 65535, else
+ * R3D_EINVAL.  Calls share the array, so calls that overlap on the GPU race.  Each call looks up
+ * the array's address in the current context; the first call on a device also loads the module
+ * there and should come before any stream capture.  Allocates no device memory. */
 int r3d_dt_limits_noalloc(const r3d_params* p, const double* const* fields,
                           const double* const* lines, double* out, void* stream);
 

@@ -10,16 +10,19 @@
 //
 // Limits and sharing:
 //  * at most kMaxBlocks partial slots: one per 32 x 8 column tile, so npx*npy is limited to
-//    ceil(npx/32) * ceil(npy/8) <= 65536 tiles (2.5 MiB of partials); larger grids are
-//    rejected with R3D_EINVAL before anything runs;
+//    ceil(npx/32) * ceil(npy/8) <= 65536 tiles (2.5 MiB of partials), and ceil(npy/8) to the
+//    65535 blocks a launch may have along y; larger grids are rejected with R3D_EINVAL before
+//    anything runs;
 //  * every call on a device uses the same array, and the array keeps the last call's partials;
 //    nothing in it has to start at zero (pass 1 writes every slot pass 2 reads), but two calls
 //    whose kernels overlap on the GPU (different streams, no ordering) race on the array;
-//  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress; make that first call before any stream capture.
+//  * every call looks up the array's device address with cudaGetSymbolAddress, with the
+//    target device current.  The first lookup in a CUDA context loads this module onto the
+//    device, so make the first call on a device before any stream capture; later lookups are
+//    host-side and cheap.  Nothing is cached across calls, so a cudaDeviceReset (which may
+//    reload the module at another address) needs no special handling.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "r3d_device.cuh"
@@ -32,13 +35,10 @@ namespace {
 
 constexpr int kTileX = 32, kTileY = 8;
 constexpr int kMaxBlocks = 65536;
-constexpr int kMaxDevices = 64;
 
 // Per-tile partial limits: min ww1, min ww2, min ww3, min vv, max Mach term.
 static __device__ __align__(256) double g_dt_partials[5 * kMaxBlocks];
 
-std::mutex g_setup_mu;
-double* g_partials_addr[kMaxDevices] = {};
 
 struct Inputs {
     const double* f[8];  // ru rv rw ro tt bx by bz (reference layout, x fastest)
@@ -156,18 +156,15 @@ __global__ void __launch_bounds__(256) dt_final_kernel(r3dk::Physics ph, const d
     }
 }
 
-// Device address of g_dt_partials on `device` (looked up once per device, that device current).
-double* partials_address(int device) {
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_partials_addr[device]) {
-        void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_dt_partials);
-        if (e != cudaSuccess || !ptr)
-            throw r3db::Error(R3D_ECUDA, std::string("cudaGetSymbolAddress(g_dt_partials): ") +
-                                             cudaGetErrorString(e));
-        g_partials_addr[device] = static_cast<double*>(ptr);
-    }
-    return g_partials_addr[device];
+// Device address of g_dt_partials in the current context (the target device is current).  Host
+// code holds only a host-side stand-in under the array's name; the kernels need this address.
+double* partials_address() {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_dt_partials);
+    if (e != cudaSuccess || !ptr)
+        throw r3db::Error(R3D_ECUDA, std::string("cudaGetSymbolAddress(g_dt_partials): ") +
+                                         cudaGetErrorString(e));
+    return static_cast<double*>(ptr);
 }
 
 }  // namespace
@@ -197,7 +194,11 @@ extern "C" int r3d_dt_limits_noalloc(const r3d_params* p, const double* const* f
             throw std::invalid_argument("grid too large for r3d_dt_limits_noalloc: " +
                                         std::to_string(bx * by) + " column tiles of 32x8, the fixed "
                                         "partials array holds " + std::to_string(kMaxBlocks));
-        if (p->gpu_id < 0 || p->gpu_id >= kMaxDevices) throw std::invalid_argument("gpu id out of range");
+        if (by > 65535)
+            throw std::invalid_argument("grid too large for r3d_dt_limits_noalloc: npy = " +
+                                        std::to_string(p->npy) + " needs " + std::to_string(by) +
+                                        " tile rows, a launch holds at most 65535");
+        if (p->gpu_id < 0) throw std::invalid_argument("gpu id out of range");
         int prev = -1;
         cudaGetDevice(&prev);
         if (prev != p->gpu_id) {
@@ -210,7 +211,7 @@ extern "C" int r3d_dt_limits_noalloc(const r3d_params* p, const double* const* f
                 if (dev >= 0) cudaSetDevice(dev);
             }
         } restore{prev != p->gpu_id ? prev : -1};
-        double* partials = partials_address(p->gpu_id);
+        double* partials = partials_address();
         const Derived d = derive(*p);
         r3dk::Physics ph{};
         ph.gamma = p->gamma;

@@ -15,7 +15,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cerrno>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -164,15 +166,16 @@ int plan_chunk_depth(int64_t tiles, int nloc, int d, int64_t slots) {
 }
 
 // z-chunk depth (planes per CTA) of the stage kernels of a handle over nloc local planes, given
-// its precision and FP64 column-tile rows; R3D_KCHUNK=<planes> in the environment overrides it.
-int stage_chunk_depth(const r3d_params& p, bool fp32, int tile_rows, int nloc) {
+// its precision, FP64 column-tile rows and the device's SM count; R3D_KCHUNK=<planes> in the
+// environment overrides it.
+int stage_chunk_depth(const r3d_params& p, bool fp32, int tile_rows, int nloc, int num_sms) {
     int depth = nloc >= 512 ? 64 : (nloc >= 256 ? 32 : 16);
     // column tiles of the stage kernel (32 x rows) and its resident CTAs per SM
     unsigned tbx = 0, tby = 0;
     if (fp32) r3dk::stage_fp32_box(&tbx, &tby);
     else r3dk::stage_fp64_box(tile_rows, &tbx, &tby);
     const int64_t tiles = (int64_t)((p.npx + 31) / 32) * ((p.npy + (int)tby - 3) / ((int)tby - 2));
-    const int64_t slots = 148 * ((fp32 ? 3 : 2) - (p.lmag && tby == 10 ? 1 : 0));
+    const int64_t slots = (int64_t)num_sms * ((fp32 ? 3 : 2) - (p.lmag && tby == 10 ? 1 : 0));
     if (p.lmag && tby == 8) {
         // 32x6 MHD tiles, two CTAs per SM: 12-plane chunks.  Measured on B200 against the
         // earlier 16/32-plane choice: 126x126x256 0.962 -> 0.922 ms per step, 252x252x256
@@ -196,10 +199,19 @@ int stage_chunk_depth(const r3d_params& p, bool fp32, int tile_rows, int nloc) {
             depth = plan_chunk_depth(tiles, nloc, depth, slots);
         }
     }
-    // R3D_KCHUNK=<planes> overrides the z-chunk depth of the stage kernels (tuning)
+    // R3D_KCHUNK=<planes> overrides the z-chunk depth of the stage kernels (tuning): a whole
+    // decimal number, clamped to [1, nloc]; anything else is ignored with a note on stderr
     if (const char* e = getenv("R3D_KCHUNK")) {
-        const int v = atoi(e);
-        if (v >= 1) depth = v;
+        char* end = nullptr;
+        errno = 0;
+        const long v = strtol(e, &end, 10);
+        if (end == e || *end != '\0' || errno == ERANGE || v < 1) {
+            fprintf(stderr, "r3d: R3D_KCHUNK='%s' is not a positive whole number; ignored\n", e);
+        } else {
+            const int k = (int)std::min<long>(v, nloc);
+            if (k != depth) fprintf(stderr, "r3d: R3D_KCHUNK overrides the z-chunk depth: %d planes (planned %d)\n", k, depth);
+            depth = k;
+        }
     }
     return depth;
 }
@@ -663,7 +675,9 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             g->geo.npz = nloc;
             g->geo.top_edge = z0 == 0 ? 1 : 0;
             g->geo.bot_edge = z0 + nloc == p->npz ? 1 : 0;
-            g->geo.tile_rows = r3dk::stage_fp64_rows(p->lmag, p->npx, p->npy, nloc);
+            cuda_ok(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device),
+                    "cudaDeviceGetAttribute(multiprocessors)");
+            g->geo.tile_rows = r3dk::stage_fp64_rows(p->lmag, p->npx, p->npy, nloc, g->num_sms);
             g->geo.pitch = (d.nx + 15) / 16 * 16;
             g->geo.plane = g->geo.pitch * d.ny;
             if (g->geo.plane * d.nz >= (int64_t(1) << 31))
@@ -737,7 +751,7 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             b.bottom_mode = p->izcon;
             b.hh = p->hh; b.theta = p->theta; b.tp = p->tp; b.tpr = p->tp;
             b.half_nx = (int)(d.nx / 2);
-            g->kchunk = stage_chunk_depth(*p, g->fp32, g->geo.tile_rows, nloc);
+            g->kchunk = stage_chunk_depth(*p, g->fp32, g->geo.tile_rows, nloc, g->num_sms);
             cuda_ok(cudaStreamSynchronize(g->stream), "create");
     } catch (...) {
         destroy_handle(g);
@@ -976,19 +990,25 @@ int r3d_gpu_memory(const r3d_gpu* g, int64_t* bytes) {
 
 void* r3d_gpu_stream(r3d_gpu* g) { return g ? (void*)g->stream : nullptr; }
 
-int r3d_gpu_plan(const r3d_params* p, int nloc, int* kchunk, int* tile_rows) {
+int r3d_gpu_plan(const r3d_params* p, int nloc, int num_sms, int* kchunk, int* tile_rows) {
     return guarded([&] {
         if (!p || !kchunk || !tile_rows) throw std::invalid_argument("r3d_gpu_plan: null argument");
         check_params(*p);
         const int n = nloc > 0 ? nloc : p->npz;
         if (n < 4 || n > p->npz) throw std::invalid_argument("r3d_gpu_plan: nloc must lie in [4, npz]");
+        int sms = num_sms;
+        if (sms <= 0) {
+            DeviceGuard dg(p->gpu_id);
+            cuda_ok(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->gpu_id),
+                    "cudaDeviceGetAttribute(multiprocessors)");
+        }
         const bool fp32 = p->precision == R3D_PREC_FP32BULK;
-        const int rows = r3dk::stage_fp64_rows(p->lmag, p->npx, p->npy, n);
+        const int rows = r3dk::stage_fp64_rows(p->lmag, p->npx, p->npy, n, sms);
         unsigned bx = 0, by = 0;
         if (fp32) r3dk::stage_fp32_box(&bx, &by);
         else r3dk::stage_fp64_box(rows, &bx, &by);
         *tile_rows = (int)by - 2;
-        *kchunk = stage_chunk_depth(*p, fp32, rows, n);
+        *kchunk = stage_chunk_depth(*p, fp32, rows, n, sms);
     });
 }
 

@@ -26,6 +26,7 @@ struct r3d_gpu {
     r3d_params p;
     r3db::Derived d;
     int device = 0;
+    int num_sms = 148;  // multiprocessors of the device (read at create)
     cudaStream_t stream = nullptr;
     r3dk::Geometry geo{};
     r3dk::Physics ph{};

@@ -102,10 +102,10 @@ struct Cells {
 }  // namespace
 
 size_t stage_fp64_smem() { return Shape<false, R3D_STAGE_TY>::smem; }
-int stage_fp64_rows(int mhd, int npx, int npy, int nloc) {
+int stage_fp64_rows(int mhd, int npx, int npy, int nloc, int num_sms) {
     if (!mhd) return R3D_STAGE_TY;
     const long tiles6 = (long)((npx + TX - 1) / TX) * ((npy + 5) / 6);
-    return tiles6 * ((nloc + 15) / 16) >= 2 * 148 ? 6 : 8;
+    return tiles6 * ((nloc + 15) / 16) >= 2L * num_sms ? 6 : 8;
 }
 void stage_fp64_box(int rows, unsigned* bx, unsigned* by) {
     *bx = SX;

@@ -101,7 +101,7 @@ def lib():
         L.r3d_gpu_download.argtypes = [vp, ctypes.POINTER(_HostStateC), ctypes.POINTER(Scalars)]
         L.r3d_gpu_destroy.argtypes = [vp]
         L.r3d_gpu_memory.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
-        L.r3d_gpu_plan.argtypes = [ctypes.POINTER(Params), ip, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.r3d_gpu_plan.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.r3d_gpu_stream.argtypes = [vp]
         L.r3d_gpu_stream.restype = vp
         L.r3d_gpu_step.argtypes = [vp, ip, ctypes.POINTER(Scalars)]
@@ -171,10 +171,11 @@ def dims(p: Params):
     return tuple(int(x.value) for x in n)
 
 
-def plan(p: Params, nloc: int = 0):
-    """(z planes per CTA, tile rows) of the stage kernels for a handle over nloc planes (0: npz)."""
+def plan(p: Params, nloc: int = 0, num_sms: int = 0):
+    """(z planes per CTA, tile rows) of the stage kernels for a handle over nloc planes (0: npz)
+    on a device with num_sms multiprocessors (0: read from device p.gpu_id)."""
     k, r = ctypes.c_int(), ctypes.c_int()
-    _check(lib().r3d_gpu_plan(ctypes.byref(p), nloc, ctypes.byref(k), ctypes.byref(r)))
+    _check(lib().r3d_gpu_plan(ctypes.byref(p), nloc, num_sms, ctypes.byref(k), ctypes.byref(r)))
     return k.value, r.value
 
 

@@ -8,6 +8,13 @@ for p in (os.path.join(ROOT, "rast-3dmhd_b200", "python"), os.path.join(ROOT, "o
     if p not in sys.path:
         sys.path.insert(0, p)
 
+# tests that re-run the reference's own sources (the Fortran LMAG block) find its checkout
+# through $R3D_REFERENCE; the build recipe knows where the build container keeps it
+if not os.environ.get("R3D_REFERENCE"):
+    import __graft_entry__
+
+    os.environ["R3D_REFERENCE"] = __graft_entry__.reference_dir()
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")

@@ -22,7 +22,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+# the reference checkout: the first argument, else $R3D_REFERENCE (no default)
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("R3D_REFERENCE", "")
 
 # hydro configurations recorded from the reference build: (name, flags, seed, nranks, steps)
 RUNS = [
@@ -41,6 +42,8 @@ def interior_sha(a: np.ndarray) -> str:
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "tests")):
+        sys.exit("usage: make_golden.py <reference checkout> (or set R3D_REFERENCE)")
     pins = {}
     inc = open(os.path.join(REF, "tests", "_ran2_ref.inc")).read()
     pins["ran2_seed62659_every1000"] = [[int(n), float(v)] for n, v in

@@ -20,7 +20,8 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 from fortran_lmag import Block, lmag_inputs  # noqa: E402
 from oracle import Oracle  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 and __name__ == "__main__" else "/root/reference"
+# the reference checkout: the first argument when run as a script, else $R3D_REFERENCE (no default)
+REF = sys.argv[1] if len(sys.argv) > 1 and __name__ == "__main__" else os.environ.get("R3D_REFERENCE", "")
 MAG = ["--lmag", "1", "--beta", "10", "--rm", "1", "--ampb", "0.1", "--bfh", "2", "--bzp", "20"]
 CASES = {
     "layer_12x10x16_seed5_3steps": (["--npx", "12", "--npy", "10", "--npz", "16"] + MAG, 5, 3),
@@ -55,6 +56,8 @@ def fortran_rhs(block, flags, seed, steps):
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "golden")):
+        sys.exit("usage: make_mhd_golden.py <reference checkout> (or set R3D_REFERENCE)")
     block = Block(os.path.join(REF, "golden", "fortran", "3dmhdsub.f"))
     data = {}
     for name, (flags, seed, steps) in CASES.items():

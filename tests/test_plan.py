@@ -4,6 +4,7 @@ import pytest
 
 import r3d_b200 as R
 
+B200_SMS = 148  # the plans below are those of a B200
 MAG = ["--lmag", "1", "--beta", "10", "--rm", "1", "--ampb", "0.1", "--bfh", "2", "--bzp", "20"]
 
 
@@ -24,7 +25,7 @@ def grid(npx, npy, npz, *extra):
         "mhd_126x126x256", "mhd_252x252x256", "mhd_64x64x128"])
 def test_plan_of_the_measured_grids(flags, want, monkeypatch):
     monkeypatch.delenv("R3D_KCHUNK", raising=False)
-    assert R.plan(R.parse(flags)) == want
+    assert R.plan(R.parse(flags), num_sms=B200_SMS) == want
 
 
 def _default_depth(nloc):
@@ -37,7 +38,7 @@ def test_hydro_depth_bounds(npx, npy, npz, monkeypatch):
     """A hydro depth never exceeds the default; a multi-wave launch adds at most one chunk and
     stays within 3/4 of the default; a single-wave launch takes a power-of-two fraction."""
     monkeypatch.delenv("R3D_KCHUNK", raising=False)
-    k, rows = R.plan(R.parse(grid(npx, npy, npz)))
+    k, rows = R.plan(R.parse(grid(npx, npy, npz)), num_sms=B200_SMS)
     d = _default_depth(npz)
     assert rows == 8 and 1 <= k <= d
     tiles = -(-npx // 32) * -(-npy // 8)
@@ -51,18 +52,32 @@ def test_hydro_depth_bounds(npx, npy, npz, monkeypatch):
 def test_slab_plan_and_errors(monkeypatch):
     monkeypatch.delenv("R3D_KCHUNK", raising=False)
     p = R.parse(grid(504, 504, 512))
-    assert R.plan(p, 512) == R.plan(p)
-    k, _ = R.plan(p, 171)                  # one of three z slabs
+    assert R.plan(p, 512, B200_SMS) == R.plan(p, 0, B200_SMS)
+    k, _ = R.plan(p, 171, B200_SMS)                  # one of three z slabs
     assert 1 <= k <= 16
     for bad in (3, 513):
         with pytest.raises(R.R3dError) as e:
-            R.plan(p, bad)
+            R.plan(p, bad, B200_SMS)
         assert e.value.code == R.R3D_EINVAL
 
 
 def test_environment_overrides_depth(monkeypatch):
     p = R.parse(grid(504, 504, 512))
     monkeypatch.setenv("R3D_KCHUNK", "40")
-    assert R.plan(p) == (40, 8)
-    monkeypatch.setenv("R3D_KCHUNK", "0")  # ignored
-    assert R.plan(p) == (62, 8)
+    assert R.plan(p, 0, B200_SMS) == (40, 8)
+    monkeypatch.setenv("R3D_KCHUNK", "9999")  # clamped to the planes held
+    assert R.plan(p, 0, B200_SMS) == (512, 8)
+    for bad in ("0", "12x", "", "-3", "abc"):  # ignored
+        monkeypatch.setenv("R3D_KCHUNK", bad)
+        assert R.plan(p, 0, B200_SMS) == (62, 8)
+
+
+def test_plan_follows_the_sm_count(monkeypatch):
+    """The plan is computed for the device's SM count: a part with fewer SMs fills its waves
+    with fewer CTAs, so a 32x32x64 grid that leaves a B200 mostly idle keeps a deeper chunk on a
+    part with 8 SMs, and an MHD grid too small for 32x6 tiles on a B200 takes them there."""
+    monkeypatch.delenv("R3D_KCHUNK", raising=False)
+    assert R.plan(R.parse(grid(32, 32, 64)), num_sms=B200_SMS) == (4, 8)
+    assert R.plan(R.parse(grid(32, 32, 64)), num_sms=8)[0] > 4
+    assert R.plan(R.parse(grid(64, 64, 128, *MAG)), num_sms=B200_SMS) == (16, 8)
+    assert R.plan(R.parse(grid(64, 64, 128, *MAG)), num_sms=16) == (12, 6)
