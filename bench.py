@@ -11,11 +11,14 @@ dataset exists for this path); the working set (15 x 1.07 GB) is far larger than
 Timing: W untimed steps, then K steps timed with CUDA events recorded by the library on the
 stream its kernels run on (every launch is bracketed, which also yields the per-kernel
 durations for the roofline); barrier + device synchronise on both sides; max over ranks.
-Under torchrun (N > 1) the domain grows to 504 x 504 x (512 N) and each rank holds one
+With N > 1 (under torchrun, or `--gpus N` alone, which starts the N ranks itself: one process
+per GPU, LOCAL_RANK set) the domain grows to 504 x 504 x (512 N) and each rank holds one
 504 x 504 x 512 z slab on its GPU (weak scaling): the ghost planes move over NCCL after every
 stage and the dt limits are all-reduced on the device every step, inside the timed region.
+`--dry-launch` starts the ranks and joins them (gloo) without GPU work: a check of the launch.
 The reference arm (--impl reference) times the reference's own CPU sources (compiled
-unmodified into oracle/_ref) on a bounded slab of the same workload, on rank 0 only.
+unmodified into oracle/_ref) on the same 504 x 504 x 512 grid, W untimed and K timed steps,
+on rank 0 only.
 """
 from __future__ import annotations
 
@@ -148,6 +151,62 @@ def dist_init():
     return world, rank, local, pg
 
 
+def spawn_ranks(n: int) -> int:
+    """`bench.py --gpus N` started without a launcher: start the N ranks here, one process per
+    GPU (RANK = LOCAL_RANK = r, WORLD_SIZE = N, rendezvous on 127.0.0.1), as torchrun would.
+    Rank 0 writes the JSON line to this process's stdout; every rank's log goes to stderr.  A
+    rank that fails or does not finish stops the others, and the exit code is nonzero."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    limit_s = float(os.environ.get("R3D_BENCH_RANK_TIMEOUT", "3600"))
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:], env=env,
+                                      stdout=_RESULT if r == 0 else sys.stderr, stderr=sys.stderr))
+    t0 = time.perf_counter()
+    rc = 0
+    while any(pr.poll() is None for pr in procs):
+        failed = [pr for pr in procs if pr.returncode not in (None, 0)]
+        if failed or time.perf_counter() - t0 > limit_s:
+            rc = failed[0].returncode if failed else 124
+            print(f"bench: rank failed or timed out (rc {rc}); stopping the other ranks", file=sys.stderr)
+            for pr in procs:
+                if pr.poll() is None:
+                    pr.kill()
+            break
+        time.sleep(0.2)
+    for pr in procs:
+        pr.wait()
+        if pr.returncode != 0 and rc == 0:
+            rc = pr.returncode
+    return rc
+
+
+def dry_launch(args, world, rank, pg) -> int:
+    """Join the ranks without GPU work: every rank reports its slab of the weak-scaling domain,
+    and the 128-byte id a real run hands to the NCCL transport goes from rank 0 to all."""
+    from r3d_b200 import dist as D
+
+    npz = GRID[2] * world
+    z0, nz = D.slab_of(npz, rank, world)
+    uid = D.share_unique_id(rank, pg, make=lambda: bytes(range(128)))
+    mine = {"rank": rank, "local_rank": int(os.environ.get("LOCAL_RANK", "0")), "slab": [z0, nz],
+            "uid_ok": uid == bytes(range(128))}
+    joined = [mine]
+    if pg is not None:
+        joined = [None] * world
+        pg.all_gather_object(joined, mine)
+    if rank == 0:
+        emit({"dry_launch": True, "n_gpus": world, "requested": args.gpus, "joined": joined,
+              "domain": [GRID[0], GRID[1], npz]})
+    return 0
+
+
 def barrier(pg):
     if pg is not None:
         pg.barrier()
@@ -163,46 +222,39 @@ def allmax(pg, x: float) -> float:
     return float(t.item())
 
 
-def cpu_reference_sample(max_seconds: float = 20.0):
-    """Time the reference CPU sources (or the oracle port when absent) on a slab of the
-    workload: full 504 x 504 plane, reduced depth, same physics and seed."""
-    import numpy as np  # noqa: F401
-
+def cpu_reference_sample(warmup: int = 1, nsteps: int = 2):
+    """Time the reference CPU sources (or the oracle port when absent) on the benchmark grid
+    itself: set-up, `warmup` untimed steps, then `nsteps` timed steps (a bounded sample, about
+    15-30 s of host time on 16 threads)."""
     ncores = os.cpu_count() or 1
-    nz = 16
-    args = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(nz), "--npey", "1"]
-    cells = GRID[0] * GRID[1] * nz
+    args = FLAGS + ["--npey", "1"]
+    cells = GRID[0] * GRID[1] * GRID[2]
     try:
         from oracle import Reference
 
         if not Reference.available():
             raise RuntimeError("reference build absent")
-        ranks = 2
-        threads = max(1, ncores // ranks)
-        # warm-up + calibration with one step, then as many as fit the budget
-        _, _, _, s1 = Reference.run(args, nranks=ranks, seed=SEED, nsteps=1, omp_threads=threads)
-        nsteps = max(1, min(10, int(max_seconds / max(s1, 1e-3))))
-        _, _, _, sec = Reference.run(args, nranks=ranks, seed=SEED, nsteps=nsteps, omp_threads=threads)
+        ranks, threads = reference_layout(ncores)
+        _, sec = Reference.time_steps(args, ranks, SEED, warmup, nsteps, threads)
         return {"value": cells * nsteps / sec / 1e6, "unit": UNIT, "cores": ranks * threads,
                 "kind": "reference",
                 "sample": f"reference CPU sources (src/*.cpp, -O2 -ffp-contract=off -fopenmp) with a "
-                          f"thread-rank MPI stand-in, {ranks} ranks x {threads} OpenMP threads, "
-                          f"grid {GRID[0]}x{GRID[1]}x{nz} (the 504x504 plane at reduced depth), "
-                          f"{nsteps} RK3 steps, seed {SEED}, host has {ncores} logical cores"}
+                          f"thread-rank MPI stand-in, {ranks} ranks x {threads} OpenMP threads, grid "
+                          f"{GRID[0]}x{GRID[1]}x{GRID[2]} (the benchmark grid), {warmup} untimed + {nsteps} "
+                          f"timed RK3 steps, seed {SEED}, host has {ncores} logical cores"}
     except Exception as e:  # oracle port as the stand-in
         from oracle import Oracle
 
-        o = Oracle(args[:6]).init(SEED)
-        o.step()
-        t0 = time.perf_counter()
-        nsteps = 0
-        while time.perf_counter() - t0 < max_seconds / 2 and nsteps < 10:
+        o = Oracle(FLAGS).init(SEED)
+        for _ in range(warmup):
             o.step()
-            nsteps += 1
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            o.step()
         sec = time.perf_counter() - t0
         return {"value": cells * nsteps / sec / 1e6, "unit": UNIT, "cores": ncores, "kind": "port",
-                "sample": f"C restatement (oracle/r3d_oracle.c, OpenMP) on {GRID[0]}x{GRID[1]}x{nz}, "
-                          f"{nsteps} steps ({e})"}
+                "sample": f"C restatement (oracle/r3d_oracle.c, OpenMP) on {GRID[0]}x{GRID[1]}x{GRID[2]}, "
+                          f"{nsteps} timed steps ({e})"}
 
 
 def side_run(R, flags, steps, warmup, bytes_per_cell, fp64_ms_per_step):
@@ -228,77 +280,100 @@ def side_run(R, flags, steps, warmup, bytes_per_cell, fp64_ms_per_step):
     return out
 
 
-def fp32_error_run(R, local, grid, steps, flags=()):
+def fp32_error_run(R, local, grid, steps, flags=(), seed=None):
     """FP32-bulk against FP64 after `steps` steps from the same initial state: per-field
-    relative L2 / Linf error on the interior, total mass and energy drift of both, and the step
-    time of both (CUDA events)."""
-    import numpy as np
-
-    base = ["--npx", str(grid[0]), "--npy", str(grid[1]), "--npz", str(grid[2]), "--seed", str(SEED),
+    relative L2 / Linf error on the interior (computed on the device, r3d_gpu_compare: no host
+    copy of either state), total mass and energy drift of both, and the step time of both (CUDA
+    events).  Both states stay on the device together (504 x 504 x 2048: 63 + 32 GB)."""
+    seed = SEED if seed is None else seed
+    base = ["--npx", str(grid[0]), "--npy", str(grid[1]), "--npz", str(grid[2]), "--seed", str(seed),
             "--gpu", str(local)] + list(flags)
-    out = {"grid": list(grid), "steps": steps, "flags": list(flags)}
-    states, totals, times = {}, {}, {}
-    for prec in ("fp64", "fp32bulk"):
-        p = R.parse(base + ["--precision", prec])
-        st = R.HostState.setup(p)
-        with R.GpuSim(p) as sim:
+    out = {"grid": list(grid), "steps": steps, "seed": seed, "flags": list(flags)}
+    p64 = R.parse(base + ["--precision", "fp64"])
+    p32 = R.parse(base + ["--precision", "fp32bulk"])
+    st = R.HostState.setup(p64)  # one host initial state for both forms
+    totals, times = {}, {}
+    with R.GpuSim(p64) as s64, R.GpuSim(p32) as s32:
+        for prec, sim in (("fp64", s64), ("fp32bulk", s32)):
             sim.upload(st)
             m0, e0 = sim.totals()
             _, tm = sim.run_timed(steps)
             m1, e1 = sim.totals()
-            sim.download(st)
-        states[prec] = st.fields
-        totals[prec] = {"mass_drift": (m1 - m0) / m0, "energy_drift": (e1 - e0) / e0}
-        times[prec] = tm["total_ms"] / steps
-    inner = (slice(1, -1), slice(1, -1), slice(1, -1))
-    err = {}
-    for n in ("ru", "rv", "rw", "ro", "tt"):
-        a = states["fp64"][n][inner]
-        b = states["fp32bulk"][n][inner]
-        d = b - a
-        err[n] = {"rel_l2": float(np.sqrt(np.sum(d * d)) / np.sqrt(np.sum(a * a))),
-                  "rel_linf": float(np.max(np.abs(d)) / np.max(np.abs(a)))}
-    out.update({"error": err, "totals": totals, "ms_per_step": times,
-                "speedup": times["fp64"] / times["fp32bulk"]})
+            totals[prec] = {"mass_drift": (m1 - m0) / m0, "energy_drift": (e1 - e0) / e0}
+            times[prec] = tm["total_ms"] / steps
+        del st
+        err = s32.compare(s64)
+    out.update({"error": err, "max_rel_l2": max(v["rel_l2"] for v in err.values()),
+                "totals": totals, "ms_per_step": times, "speedup": times["fp64"] / times["fp32bulk"],
+                "mcell_updates_per_s": {k: grid[0] * grid[1] * grid[2] / (v / 1e3) / 1e6 for k, v in times.items()}})
     return out
 
 
+# BASELINE configuration 4: FP32-bulk 504 x 504 x 2048 with the reference's plume top boundary
+# (tp 2, itcon 1; src/bcon.cpp:43-70), seed 11, 50 steps, FP64 alongside
+PLUME = ["--tp", "2", "--tc", "0", "--xp", "10", "--yp", "10", "--zp", "0", "--hh", "1"]
+
+
 def adjoint_run(R, local):
-    """Wall time of the discrete adjoint on the MHD 64x64x128 case: record 200 steps with a
-    checkpoint every 20, then the checkpointed reverse sweep (seed: d(kinetic energy)/dX)."""
+    """Time of the discrete adjoint on the MHD 64x64x128 case: record 200 steps with a
+    checkpoint every 20, then the checkpointed reverse sweep (seed: d(kinetic energy)/dX).
+    CUDA events on the library's stream bracket each call (device time, host gaps included);
+    the wall clock around the synchronous calls is reported beside them."""
     import numpy as np
+    import torch
 
     p = R.parse(["--npx", "64", "--npy", "64", "--npz", "128", "--lmag", "1", "--beta", "10", "--rm", "1",
                  "--ampb", "0.1", "--bfh", "2", "--bzp", "20", "--seed", "5", "--gpu", str(local)])
     st = R.HostState.setup(p)
     with R.GpuSim(p) as sim:
+        stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         sim.upload(st)
         sim.adjoint_record(20, 20)  # warm-up (allocates the workspace)
-        sim.upload(st)
-        t0 = time.perf_counter()
-        sim.adjoint_record(200, 20)
-        t1 = time.perf_counter()
         fin = st.copy()
         sim.download(fin)
         seed = {n: np.zeros_like(a) for n, a in fin.fields.items()}
+        sim.adjoint_backward(seed)  # warm-up of the reverse kernels
+        sim.upload(st)
+        torch.cuda.synchronize(local)
+        t0 = time.perf_counter()
+        ev[0].record(stream)
+        sim.adjoint_record(200, 20)
+        ev[1].record(stream)
+        t1 = time.perf_counter()
+        sim.download(fin)
         ro = fin.fields["ro"]
         for n in ("ru", "rv", "rw"):
             seed[n] = fin.fields[n] / ro
         seed["ro"] = -0.5 * (fin.fields["ru"] ** 2 + fin.fields["rv"] ** 2 + fin.fields["rw"] ** 2) / ro ** 2
+        torch.cuda.synchronize(local)
         t2 = time.perf_counter()
+        ev[2].record(stream)
         sim.adjoint_backward(seed)
+        ev[3].record(stream)
         t3 = time.perf_counter()
+        torch.cuda.synchronize(local)
+        fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
         mem = sim.adjoint_memory_bytes
     cells = 64 * 64 * 128
     return {"grid": [64, 64, 128], "steps": 200, "checkpoint_every": 20,
-            "forward_record_ms": (t1 - t0) * 1e3, "backward_ms": (t3 - t2) * 1e3,
-            "backward_over_forward": (t3 - t2) / (t1 - t0),
-            "adjoint_mcell_steps_per_s": cells * 200 / (t3 - t2) / 1e6, "adjoint_device_bytes": mem,
-            "note": "wall clock around synchronous C ABI calls (host seed upload and gradient download "
-                    "included in backward_ms)"}
+            "forward_record_ms": fwd_ms, "backward_ms": bwd_ms, "backward_over_forward": bwd_ms / fwd_ms,
+            "wall_ms": {"forward_record": (t1 - t0) * 1e3, "backward": (t3 - t2) * 1e3},
+            "adjoint_mcell_steps_per_s": cells * 200 / (bwd_ms / 1e3) / 1e6, "adjoint_device_bytes": mem,
+            "note": "CUDA events on the library stream around each synchronous C ABI call (the "
+                    "backward includes its seed upload and gradient download); wall_ms: host clock"}
+
+
+def reference_layout(ncores: int):
+    """Thread-ranks x OpenMP threads of the reference CPU run on ncores host threads (the
+    reference needs npez >= 2 ranks)."""
+    ranks = 2
+    return ranks, max(1, ncores // ranks)
 
 
 def run_reference_arm(args, world, rank, pg):
+    """The reference's own CPU implementation (src/*.cpp compiled unmodified, thread-rank MPI
+    stand-in, OpenMP) on the benchmark grid: set-up, W untimed steps, K timed steps."""
     if rank != 0:
         return 0
     base = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
@@ -311,21 +386,20 @@ def run_reference_arm(args, world, rank, pg):
                   "unavailable": "reference CPU build oracle/_ref/libr3dref.so not present"})
             return 0
         ncores = os.cpu_count() or 1
-        nz = 16
-        fl = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(nz), "--npey", "1"]
-        cells = GRID[0] * GRID[1] * nz
-        ranks, threads = 2, max(1, ncores // 2)
-        Reference.run(fl, nranks=ranks, seed=SEED, nsteps=max(1, args.warmup // 3), omp_threads=threads)
-        nsteps = max(1, min(args.steps, 10))
-        _, _, _, sec = Reference.run(fl, nranks=ranks, seed=SEED, nsteps=nsteps, omp_threads=threads)
-        v = cells * nsteps / sec / 1e6
+        fl = FLAGS + ["--npey", "1"]
+        cells = GRID[0] * GRID[1] * GRID[2]
+        ranks, threads = reference_layout(ncores)
+        sc, sec = Reference.time_steps(fl, ranks, SEED, args.warmup, args.steps, threads)
+        v = cells * args.steps / sec / 1e6
         sample = (f"reference CPU sources compiled unmodified (-O2 -ffp-contract=off -fopenmp), "
-                  f"{ranks} thread-ranks x {threads} OpenMP threads, grid {GRID[0]}x{GRID[1]}x{nz} "
-                  f"(504x504 plane, reduced depth), {nsteps} timed RK3 steps, seed {SEED}")
-        out = {**base, "value": v, "ms_per_step": sec / nsteps * 1e3, "scaling": "weak", "vs_baseline": None,
-               "dtype": "f64", "data": "synthetic",
+                  f"{ranks} thread-ranks x {threads} OpenMP threads on {ncores} host threads, grid "
+                  f"{GRID[0]}x{GRID[1]}x{GRID[2]} (the full benchmark grid), {args.warmup} untimed + "
+                  f"{args.steps} timed RK3 steps, seed {SEED}")
+        out = {**base, "value": v, "ms_per_step": sec / args.steps * 1e3, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                "config": {"workload": f"FP64 hydro {GRID[0]}x{GRID[1]}x{GRID[2]} default physics seed {SEED}",
-                          "sample_grid": f"{GRID[0]}x{GRID[1]}x{nz}"},
+                          "grid": list(GRID)},
+               "final_dt": sc["dt"],
                "cpu_baseline": {"value": v, "unit": UNIT, "cores": ranks * threads, "kind": "reference",
                                 "sample": sample},
                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -354,7 +428,8 @@ def main():
     sys.stdout.flush()
     _RESULT = os.fdopen(os.dup(1), "w")
     os.dup2(2, 1)
-    os.environ.setdefault("NCCL_DEBUG", "WARN")
+    # NCCL's communicator lines (rank counts) go to stderr with the rest of the log
+    os.environ.setdefault("NCCL_DEBUG", "INFO")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=60)
@@ -374,17 +449,16 @@ def main():
                     help="only measure FP32-bulk against FP64 on this grid after STEPS steps and print it")
     ap.add_argument("--plume", action="store_true",
                     help="with --fp32-error: plume forcing tp=2 tc=0 xp=yp=10 zp=0 hh=1, seed 11")
+    ap.add_argument("--dry-launch", action="store_true",
+                    help="start and join the ranks (gloo) and report them, without GPU work")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args.gpus)
     if args.fp32_error:
         import r3d_b200 as R
 
-        global SEED
-        fl = []
-        if args.plume:
-            SEED = 11
-            fl = ["--tp", "2", "--tc", "0", "--xp", "10", "--yp", "10", "--zp", "0", "--hh", "1"]
         g = args.fp32_error
-        emit(fp32_error_run(R, 0, g[:3], g[3], fl))
+        emit(fp32_error_run(R, 0, g[:3], g[3], PLUME if args.plume else (), seed=11 if args.plume else None))
         return 0
     global GRID, FLAGS
     if args.grid:
@@ -393,6 +467,16 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_init()
+    if world != args.gpus:
+        print(f"bench: --gpus {args.gpus} but {world} ranks joined", file=sys.stderr)
+        if pg is not None:
+            pg.destroy_process_group()
+        return 2
+    if args.dry_launch:
+        rc = dry_launch(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return rc
     if args.impl == "reference":
         rc = run_reference_arm(args, world, rank, pg)
         if pg is not None:
@@ -486,6 +570,8 @@ def main():
                                                  max(args.steps, 20), args.warmup, 640.0, None)
         extra["adjoint_mhd_64x64x128"] = adjoint_run(R, local)
         extra["fp32bulk_error_504x504x512_100steps"] = fp32_error_run(R, local, GRID, 100)
+        extra["config4_fp32bulk_plume_504x504x2048_50steps"] = fp32_error_run(R, local, (504, 504, 2048), 50,
+                                                                              PLUME, seed=11)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu = cpu_reference_sample()

@@ -204,6 +204,13 @@ int r3d_gpu_run_timed(r3d_gpu* g, int nsteps, r3d_scalars* sc, r3d_timing* tm);
 /* Volume sums of rho and of the total energy proxy over the interior, accumulated in FP64 on
  * the device (mass = sum rho, energy = sum (rho*T*cv + 0.5*(ru^2+rv^2+rw^2)/rho)). */
 int r3d_gpu_totals(r3d_gpu* g, double* mass, double* energy);
+/* Error norms of a's current state against ref's over the interior cells, computed on the
+ * device (no counterpart in the reference; it measures the FP32-bulk form against FP64 on grids
+ * whose host copies would not fit in host memory).  For each field q of ref (ru rv rw ro tt,
+ * then bx by bz with lmag): out[4q..4q+3] = sum (a-ref)^2, sum ref^2, max |a-ref|, max |ref|.
+ * Either handle may hold either precision (FP32-bulk rho and T compared as full values); both
+ * must hold the same grid and slab on the same device.  Deterministic (fixed summation order). */
+int r3d_gpu_compare(const r3d_gpu* a, const r3d_gpu* ref, double* out);
 
 /* ---- discrete adjoint of the RK3 step (FP64; no counterpart in the reference) ----
  * Reverse-mode derivative of exactly the map r3d_gpu_run computes (FLUXES, the stage update,

@@ -174,6 +174,8 @@ class Reference:
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
             lib.ref_last_error.restype = ctypes.c_char_p
             lib.ref_ran2.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+            lib.ref_time.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
             cls._lib = lib
         return cls._lib
 
@@ -206,6 +208,20 @@ class Reference:
                 lines[nm] = out1[off:off + n1].copy()
                 off += n1
         return fields, lines, dict(zip(SCALARS, sc.tolist())), float(secs[0])
+
+    @classmethod
+    def time_steps(cls, args: Sequence[str], nranks: int, seed: int, warmup: int, nsteps: int,
+                   omp_threads: int):
+        """Set-up, `warmup` untimed and `nsteps` timed reference steps without gathering the
+        state; returns (scalars, seconds of the timed steps)."""
+        sc = np.zeros(7)
+        secs = np.zeros(1)
+        arr, n = _argv(args)
+        rc = cls.lib().ref_time(arr, n, nranks, seed, warmup, nsteps, omp_threads, sc.ctypes.data,
+                                secs.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(cls.lib().ref_last_error().decode())
+        return dict(zip(SCALARS, sc.tolist())), float(secs[0])
 
     @classmethod
     def ran2(cls, seed: int, n: int) -> np.ndarray:

@@ -46,6 +46,7 @@ struct Job {
     int last_stages = 3;
     int omp_threads = 1;
     int fluxes_only = 0;  // after nsteps, run one FLUXES and return FU..FT in place of state
+    int warmup = 0;       // untimed steps before the timed nsteps (timing runs)
     // outputs (global arrays, may be null)
     double* out3d = nullptr;   // 8 x NX*NY*NZ : ru rv rw ro tt bx by bz (or fu fv fw fr ft ...)
     double* out1d = nullptr;   // 14 x (NX | NY | NZ) packed: exx.. (NX) wyy.. (NY) zee.. (NZ) rkapa dkapa (NZ)
@@ -170,6 +171,7 @@ void rank_main(Job& job, int rank) {
     s.timi = 0.0;
     r3d::communicate(MPI_COMM_WORLD, p, t, s);
 
+    for (int n = 1; n <= job.warmup; ++n) r3d::step(3, MPI_COMM_WORLD, p, d, t, s);
     double wbuf[1] = {0.0}, wout[1];
     MPI_Allreduce(wbuf, wout, 1, MPI_DOUBLE, MPI_MIN, MPI_COMM_WORLD);
     auto t0 = std::chrono::steady_clock::now();
@@ -203,27 +205,8 @@ void rank_main(Job& job, int rank) {
 
 std::string g_last_error;
 
-}  // namespace
-
-extern "C" {
-
-// Run the reference CPU step.  args/nargs are reference CLI flags (src/params.cpp:113-224).
-// Returns 0 on success, nonzero on failure (message via ref_last_error).
-int ref_run(const char** args, int nargs, int nranks, int seed, int nsteps, int last_stages,
-            int omp_threads, int fluxes_only, double* out3d, double* out1d, double* scalars,
-            double* seconds) {
-    Job job;
-    for (int i = 0; i < nargs; ++i) job.args.emplace_back(args[i]);
-    job.nranks = nranks;
-    job.seed = seed;
-    job.nsteps = nsteps;
-    job.last_stages = last_stages;
-    job.omp_threads = omp_threads;
-    job.fluxes_only = fluxes_only;
-    job.out3d = out3d;
-    job.out1d = out1d;
-    job.scalars = scalars;
-    job.seconds = seconds;
+int run_job(Job& job) {
+    const int nranks = job.nranks;
     r3d_shim_world_init(nranks);
     std::vector<std::thread> th;
     std::vector<std::string> errs(nranks);
@@ -245,6 +228,46 @@ int ref_run(const char** args, int nargs, int nranks, int seed, int nsteps, int 
     for (auto& e : errs)
         if (!e.empty()) g_last_error = e;
     return g_last_error.empty() ? 0 : 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Run the reference CPU step.  args/nargs are reference CLI flags (src/params.cpp:113-224).
+// Returns 0 on success, nonzero on failure (message via ref_last_error).
+int ref_run(const char** args, int nargs, int nranks, int seed, int nsteps, int last_stages,
+            int omp_threads, int fluxes_only, double* out3d, double* out1d, double* scalars,
+            double* seconds) {
+    Job job;
+    for (int i = 0; i < nargs; ++i) job.args.emplace_back(args[i]);
+    job.nranks = nranks;
+    job.seed = seed;
+    job.nsteps = nsteps;
+    job.last_stages = last_stages;
+    job.omp_threads = omp_threads;
+    job.fluxes_only = fluxes_only;
+    job.out3d = out3d;
+    job.out1d = out1d;
+    job.scalars = scalars;
+    job.seconds = seconds;
+    return run_job(job);
+}
+
+// Timing run: set-up, `warmup` untimed steps, then `nsteps` timed steps (wall time of the
+// stepping loop on rank 0 into *seconds); only the scalars are returned (no gather).
+int ref_time(const char** args, int nargs, int nranks, int seed, int warmup, int nsteps, int omp_threads,
+             double* scalars, double* seconds) {
+    Job job;
+    for (int i = 0; i < nargs; ++i) job.args.emplace_back(args[i]);
+    job.nranks = nranks;
+    job.seed = seed;
+    job.warmup = warmup;
+    job.nsteps = nsteps;
+    job.omp_threads = omp_threads;
+    job.scalars = scalars;
+    job.seconds = seconds;
+    return run_job(job);
 }
 
 const char* ref_last_error(void) { return g_last_error.c_str(); }

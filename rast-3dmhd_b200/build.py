@@ -20,7 +20,7 @@ HOST_SRCS = ["host/params.cpp", "host/setup.cpp"]
 # FMA contraction: off everywhere the FP64 result must equal the reference CPU build; on for
 # the FP32-bulk kernels, which carry no bit-exactness contract.
 FMAD_ON = {"csrc/step_fp32.cu", "csrc/bcon_fp32.cu"}
-CU_SRCS = ["csrc/step_fp64.cu", "csrc/bcon.cu", "csrc/step_fp32.cu", "csrc/bcon_fp32.cu", "csrc/r3d_gpu.cu", "csrc/dt_noalloc.cu", "csrc/adjoint.cu", "csrc/halo.cu", "csrc/mesh.cu"]
+CU_SRCS = ["csrc/step_fp64.cu", "csrc/bcon.cu", "csrc/step_fp32.cu", "csrc/bcon_fp32.cu", "csrc/r3d_gpu.cu", "csrc/dt_noalloc.cu", "csrc/adjoint.cu", "csrc/halo.cu", "csrc/mesh.cu", "csrc/compare.cu"]
 LIB = os.path.join(PKG, "lib", "librast3d_b200.so")
 BIN = os.path.join(PKG, "bin", "r3d_b200")
 

@@ -109,6 +109,7 @@ def lib():
         L.r3d_gpu_enqueue.argtypes = [vp, ip]
         L.r3d_gpu_run_timed.argtypes = [vp, ip, ctypes.POINTER(Scalars), ctypes.POINTER(Timing)]
         L.r3d_gpu_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.r3d_gpu_compare.argtypes = [vp, vp, ctypes.c_void_p]
         L.r3d_gpu_debug_tma_extra.argtypes = [vp, ctypes.c_uint]
         L.r3d_gpu_debug_dt_filter.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         L.r3d_gpu_fluxes.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
@@ -329,6 +330,19 @@ class GpuSim:
         m, e = ctypes.c_double(), ctypes.c_double()
         _check(lib().r3d_gpu_totals(self.h, ctypes.byref(m), ctypes.byref(e)))
         return m.value, e.value
+
+    def compare(self, ref: "GpuSim") -> Dict[str, Dict[str, float]]:
+        """Error of this state against ref's, on the device: per field rel_l2 =
+        ||self - ref|| / ||ref|| and rel_linf = max|self - ref| / max|ref| over the interior."""
+        names = ["ru", "rv", "rw", "ro", "tt"] + (["bx", "by", "bz"] if self.p.lmag else [])
+        out = np.zeros(4 * len(names))
+        _check(lib().r3d_gpu_compare(self.h, ref.h, out.ctypes.data))
+        res = {}
+        for q, n in enumerate(names):
+            sd, sr, md, mr = out[4 * q:4 * q + 4]
+            res[n] = {"rel_l2": float(np.sqrt(sd) / np.sqrt(sr)) if sr > 0 else float(np.sqrt(sd)),
+                      "rel_linf": float(md / mr) if mr > 0 else float(md)}
+        return res
 
     def fluxes(self) -> Dict[str, np.ndarray]:
         """FLUXES of the current state: fu fv fw fr ft (+ w1 w2 w3), shapes (NZ, NY, NX)."""

@@ -74,3 +74,62 @@ def test_fp32bulk_upload_download_roundtrip_and_determinism():
     assert s1 == s2
     for n in FIELDS:
         assert np.array_equal(o1.fields[n], o2.fields[n]), n
+
+
+@pytest.mark.gpu
+def test_device_compare_equals_host_norms():
+    """r3d_gpu_compare (the on-device error norms the large-grid checks use) against numpy on
+    the downloaded states: FP32-bulk vs FP64 and FP64 vs FP64 after a few steps."""
+    flags = ["--npx", "40", "--npy", "24", "--npz", "32", "--seed", "4"]
+    p64, p32 = R.parse(flags), R.parse(flags + ["--precision", "fp32bulk"])
+    st = R.HostState.setup(p64)
+    with R.GpuSim(p64) as a, R.GpuSim(p32) as b, R.GpuSim(p64) as c:
+        for sim, n in ((a, 5), (b, 5), (c, 4)):
+            sim.upload(st)
+            sim.run(n)
+        got = {"fp32": b.compare(a), "fp64": c.compare(a)}
+        host = {}
+        for k, sim in (("a", a), ("b", b), ("c", c)):
+            h = R.HostState.empty(p64)
+            sim.download(h)
+            host[k] = h
+    for key, other in (("fp32", "b"), ("fp64", "c")):
+        for n in FIELDS:
+            x = host["a"].fields[n][1:-1, 1:-1, 1:-1]
+            y = host[other].fields[n][1:-1, 1:-1, 1:-1]
+            l2 = np.linalg.norm(y - x) / np.linalg.norm(x)
+            li = np.abs(y - x).max() / np.abs(x).max()
+            assert got[key][n]["rel_l2"] == pytest.approx(l2, rel=1e-9, abs=1e-300), (key, n)
+            assert got[key][n]["rel_linf"] == pytest.approx(li, rel=1e-12, abs=1e-300), (key, n)
+    assert all(v["rel_l2"] > 0 for v in got["fp64"].values())  # one step apart: not identical
+
+
+@pytest.mark.gpu
+def test_config4_plume_504x504x2048_fp32bulk_vs_fp64():
+    """The FP32-bulk benchmark configuration: 504 x 504 x 2048 with the reference's plume top
+    boundary (tp 2, itcon 1, Gaussian at xp = yp = 10, zp 0, hh 1; src/bcon.cpp:43-70), seed 11,
+    50 steps, the FP64 form alongside from the same initial state (63 + 32 GB on the device).
+    Errors are computed on the device; bar as above: rel L2 <= 1e-5, rel Linf <= 1e-4 per field,
+    equal drift of mass and energy, and the FP32-bulk step faster."""
+    flags = ["--npx", "504", "--npy", "504", "--npz", "2048", "--seed", "11", "--tp", "2", "--tc", "0",
+             "--xp", "10", "--yp", "10", "--zp", "0", "--hh", "1"]
+    p64, p32 = R.parse(flags), R.parse(flags + ["--precision", "fp32bulk"])
+    st = R.HostState.setup(p64)
+    drift, ms = {}, {}
+    with R.GpuSim(p64) as a, R.GpuSim(p32) as b:
+        for k, sim in (("fp64", a), ("fp32", b)):
+            sim.upload(st)
+            m0, e0 = sim.totals()
+            sc, tm = sim.run_timed(50)
+            m1, e1 = sim.totals()
+            drift[k] = ((m1 - m0) / m0, (e1 - e0) / e0)
+            ms[k] = tm["total_ms"] / 50
+            assert sc["nit"] == 50
+        del st
+        err = b.compare(a)
+    for n in FIELDS:
+        assert err[n]["rel_l2"] <= 1e-5, (n, err[n])
+        assert err[n]["rel_linf"] <= 1e-4, (n, err[n])
+    for q in (0, 1):
+        assert abs(drift["fp64"][q] - drift["fp32"][q]) <= 1e-9, (q, drift)
+    assert ms["fp32"] < ms["fp64"], ms
