@@ -115,6 +115,12 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out);
 int r3d_gpu_create_slab(const r3d_params* p, int z0, int nz, r3d_gpu** out);
 int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc);
 int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc);
+/* The RK accumulators (the reference's ZRU ZRV ZRW ZRO ZTT, + ZBX ZBY ZBZ with lmag: the
+ * SimState fields gpu_download fills, include/fields.hpp:118,123) into z[0..nfields-1] (NULL
+ * entries skipped), host arrays in the layout of r3d_gpu_download.  Interior cells; after a
+ * full step they hold X + zeta_2 dt F of the second stage, as after the reference's step()
+ * (src/step.cpp:240-246).  Ghost cells are not maintained (0 or stale). */
+int r3d_gpu_download_accumulators(r3d_gpu* g, double* const* z);
 int r3d_gpu_destroy(r3d_gpu* g);
 /* ---- z slabs over several processes (replaces the MPI/NCCL halo exchange of
  *      src/communicate.cpp:70-182 and the dt MPI_Allreduce of src/step.cpp:224) ----

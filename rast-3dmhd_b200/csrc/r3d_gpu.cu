@@ -123,6 +123,17 @@ __global__ void from_fp32_kernel(double* out, const float* in, int64_t pitch, in
     }
 }
 
+// RK accumulator of the FP32-bulk form (stored one column left: element (i,j,k) at
+// k*plane + j*pitch + i - 1) to the reference layout in FP64, interior columns only (i = 0: 0).
+__global__ void z_from_fp32_kernel(double* out, const float* in, int64_t pitch, int64_t plane, int64_t nx,
+                                   int64_t ny, int64_t nz, const double* bg) {
+    const int64_t n = nx * ny * nz;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+        out[c] = i == 0 ? 0.0 : (bg ? bg[k] : 0.0) + (double)in[k * plane + j * pitch + i - 1];
+    }
+}
+
 // Estimated length of one stage launch over `tiles` column tiles x z-chunks of depth k, in
 // plane loads: list scheduling of the CTAs in launch order (the chunk is the slowest block
 // index, so the last chunk's CTAs run last) onto `slots` resident CTA slots, each CTA costing
@@ -906,6 +917,35 @@ int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc) {
             }
         }
         pull_scalars(g, sc);
+    });
+}
+
+int r3d_gpu_download_accumulators(r3d_gpu* g, double* const* z) {
+    return guarded([&] {
+        if (!g || !z) throw std::invalid_argument("null argument");
+        if (!g->uploaded) throw Error(R3D_ESTATE, "download before upload");
+        DeviceGuard dg(g->device);
+        Range r("r3d.download");
+        const Derived& d = g->d;
+        if (g->fp32) {
+            Fp64Staging stg(g);
+            for (int q = 0; q < 5; ++q) {
+                if (!z[q]) continue;
+                z_from_fp32_kernel<<<stg.blocks(), 256, 0, g->stream>>>(stg.buf, g->Z32[q], g->geo.pitch, g->geo.plane,
+                                                                        d.nx, d.ny, d.nz, stg.bg(q));
+                cuda_ok(cudaGetLastError(), "download accumulators32");
+                cuda_ok(cudaMemcpyAsync(z[q], stg.buf, stg.n * sizeof(double), cudaMemcpyDeviceToHost, g->stream),
+                        "download accumulators32");
+            }
+        } else {
+            for (int q = 0; q < g->nfields; ++q) {
+                if (!z[q]) continue;
+                cuda_ok(cudaMemcpy2DAsync(z[q], d.nx * sizeof(double), g->Z[q], g->geo.pitch * sizeof(double),
+                                          d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyDeviceToHost, g->stream),
+                        "download accumulators");
+            }
+        }
+        cuda_ok(cudaStreamSynchronize(g->stream), "download accumulators");
     });
 }
 

@@ -39,7 +39,8 @@ struct r3d_gpu {
     double* Z[r3dk::kMaxFields] = {};
     // FP32-bulk state (precision == R3D_PREC_FP32BULK): momenta and rho', T' deviations
     bool fp32 = false;
-    float* X32[2][5] = {};
+    float* X32[2][5] = {};     // element (0,0,0) of each FP32 state array
+    float* X32mem[2][5] = {};  // the allocations (X32 = X32mem + 1)
     float* Z32[5] = {};
     r3dk::Background bg{};
     void* bg_buf = nullptr;

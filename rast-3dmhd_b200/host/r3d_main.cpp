@@ -52,6 +52,7 @@ double derived(const r3d_params& p, const char* name) {
 struct HostState {
     int64_t nx = 0, ny = 0, nz = 0;
     std::vector<double> f[8];     // ru rv rw ro tt bx by bz
+    std::vector<double> z[8];     // the RK accumulators zru .. ztt, zbx zby zbz (0 before a step)
     std::vector<double> line[14]; // exx dxxdx d2xxdx2 ddx wyy dyydy d2yydy2 ddy zee dzzdz d2zzdz2 ddz rkapa dkapa
     r3d_host_state view{};
 
@@ -59,6 +60,7 @@ struct HostState {
         r3d_dims(&p, &nx, &ny, &nz);
         const size_t n = (size_t)(nx * ny * nz);
         for (auto& a : f) a.assign(n, 0.0);
+        for (auto& a : z) a.assign(n, 0.0);
         const int64_t len[14] = {nx, nx, nx, nx, ny, ny, ny, ny, nz, nz, nz, nz, nz, nz};
         for (int q = 0; q < 14; ++q) line[q].assign((size_t)len[q], 0.0);
         double** fp[8] = {&view.ru, &view.rv, &view.rw, &view.ro, &view.tt, &view.bx, &view.by, &view.bz};
@@ -90,9 +92,10 @@ double initial_dt(const r3d_params& p, const HostState& s) {
 }
 
 // gstate dump, src/main.cpp:42-93: magic, counts, 13-int header, 27 scalars, 27 3D arrays and
-// 14 1D arrays each preceded by its int64 length, int64 -1.  The 19 work arrays the reference
-// keeps on its GPU (uu vv ww, fu..ft, zru..ztt, ww1..ww3, zbx..zbz) are not held by this
-// implementation between steps and are written as zeros.
+// 14 1D arrays each preceded by its int64 length, int64 -1.  The RK accumulators zru..ztt and
+// zbx..zbz are the device's (r3d_gpu_download_accumulators, interior cells).  The other work
+// arrays of the reference's dump (uu vv ww, fu..ft, ww1..ww3: temporaries of its FLUXES sweeps)
+// do not exist in the fused kernels and are written as zeros.
 void write_gstate(const r3d_params& p, const HostState& s, const r3d_scalars& sc, const char* tag, int iter) {
     char fname[256];
     std::snprintf(fname, sizeof fname, "gstate.%s.%03d.%04d", tag, 0, iter);
@@ -117,13 +120,15 @@ void write_gstate(const r3d_params& p, const HostState& s, const r3d_scalars& sc
     w(scal, sizeof scal);
     // the reference's field order: ru rv rw ro tt uu vv ww fu fv fw fr ft zru zrv zrw zro ztt
     // ww1 ww2 ww3 bx by bz zbx zby zbz
-    const int order[27] = {0, 1, 2, 3, 4, -1, -1, -1, -1, -1, -1, -1, -1, -1,
-                           -1, -1, -1, -1, -1, -1, -1, 5, 6, 7, -1, -1, -1};
+    // (primaries 0-7, accumulators 8-15, -1: not kept)
+    const int order[27] = {0, 1, 2, 3, 4, -1, -1, -1, -1, -1, -1, -1, -1, 8,
+                           9, 10, 11, 12, -1, -1, -1, 5, 6, 7, 13, 14, 15};
     const int64_t cnt = s.nx * s.ny * s.nz;
     std::vector<double> zeros((size_t)cnt, 0.0);
     for (int q = 0; q < 27; ++q) {
         w(&cnt, 8);
-        w(order[q] >= 0 ? s.f[order[q]].data() : zeros.data(), (size_t)cnt * 8);
+        const int o = order[q];
+        w(o < 0 ? zeros.data() : (o < 8 ? s.f[o].data() : s.z[o - 8].data()), (size_t)cnt * 8);
     }
     for (int q = 0; q < 14; ++q) {
         const int64_t c = (int64_t)s.line[q].size();
@@ -200,6 +205,9 @@ int main(int argc, char** argv) {
         if (should_log(sc.nit, nk)) {
             if (should_dump(sc.nit, nk)) {
                 check(r3d_gpu_download(g, &s.view, nullptr), "r3d_gpu_download");
+                double* zp[8];
+                for (int q = 0; q < 8; ++q) zp[q] = s.z[q].data();
+                check(r3d_gpu_download_accumulators(g, zp), "r3d_gpu_download_accumulators");
                 write_gstate(p, s, sc, "step", sc.nit);
             }
             const double wall = wall_since();

@@ -5,8 +5,9 @@ Layout (little endian): int32 magic 1129928788, int32 nf = 27, int32 n1 = 14; a 
 (nx, ny, nz, three zeros, nit, lmag, ixcon, iycon, izcon, itcon, ibcon); 27 doubles (dt timc
 timt timi umach re repr cv ocv ore theta grav rkapst orm rm obeta omx omz sf ampt, a zero, hx h2x
 hy h2y hz h2z); nf 3D arrays and n1 1D arrays, each an int64 element count followed by the
-doubles; int64 -1.  3D arrays are (nz, ny, nx) with x fastest.  The driver holds no work
-arrays between steps, so uu..ft, zru..ztt, ww1..ww3 and zbx..zbz are written as zeros.
+doubles; int64 -1.  3D arrays are (nz, ny, nx) with x fastest.  The r3d_b200 driver writes the
+RK accumulators zru..ztt and zbx..zbz from the device (interior cells); the FLUXES temporaries
+uu..ft and ww1..ww3 do not exist in the fused kernels and are written as zeros.
 """
 from __future__ import annotations
 
