@@ -114,6 +114,14 @@ int r3d_gpu_create(const r3d_params* p, r3d_gpu** out);
  * planes as constants; r3d_gpu_halo_init connects the slabs of several processes. */
 int r3d_gpu_create_slab(const r3d_params* p, int z0, int nz, r3d_gpu** out);
 int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc);
+/* The initial state built on the device (replaces r3d_setup_host + r3d_gpu_upload; the set-up
+ * of src/main.cpp:134-154, src/static_ic.cpp:24-161): metric lines, static columns and the
+ * magnetic layer from the host (1D), the fields filled by kernels, and the seeded temperature
+ * perturbation streamed plane by plane - RAN2 is one sequential chain, drawn on the host into a
+ * small pinned ring while the device applies the planes before.  No host 3D arrays.  The state
+ * (and *sc: zeros and tb) is bit-identical to r3d_setup_host followed by r3d_gpu_upload; works
+ * for slab handles (the draws of the planes above the slab are skipped) and both precisions. */
+int r3d_gpu_setup(r3d_gpu* g, r3d_scalars* sc);
 int r3d_gpu_download(r3d_gpu* g, r3d_host_state* st, r3d_scalars* sc);
 /* The RK accumulators (the reference's ZRU ZRV ZRW ZRO ZTT, + ZBX ZBY ZBZ with lmag: the
  * SimState fields gpu_download fills, include/fields.hpp:118,123) into z[0..nfields-1] (NULL

@@ -21,6 +21,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <queue>
 #include <string>
 #include <vector>
@@ -120,6 +121,60 @@ __global__ void from_fp32_kernel(double* out, const float* in, int64_t pitch, in
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
         out[c] = (bg ? bg[k] : 0.0) + (double)in[k * plane + j * pitch + i];
+    }
+}
+
+// Initial condition on the device (src/static_ic.cpp:24-161), one field in the reference layout
+// (contiguous nx*ny*nz, local planes): kind 0 zero (momenta, By, Bz), 1 the temperature column,
+// 2 the density column (with LMAG less Bx^2/T*obeta, the layer correction, on the domain's
+// interior planes: local plane k is global plane z0 + k of nzg), 3 the magnetic layer Bx.  Every
+// cell of a plane, x/y ghosts included, takes the plane's value, as the host set-up leaves them
+// after its periodic ghost copy.
+__global__ void ic_field_kernel(double* out, int64_t nx, int64_t ny, int64_t nz, int kind, const double* col_t,
+                                const double* col_r, const double* bfac, double obeta, int lmag, int64_t z0,
+                                int64_t nzg) {
+    const int64_t n = nx * ny * nz;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = c / (nx * ny);
+        double v = 0.0;
+        if (kind == 1) {
+            v = col_t[k];
+        } else if (kind == 2) {
+            v = col_r[k];
+            if (lmag && z0 + k >= 1 && z0 + k <= nzg - 2)
+                v = v - bfac[k] * bfac[k] / col_t[k] * obeta;  // src/static_ic.cpp:104-107
+        } else if (kind == 3) {
+            v = bfac[k];
+        }
+        out[c] = v;
+    }
+}
+
+// Temperature perturbation of one interior plane (src/static_ic.cpp:114-159): T *= 1 + ampt *
+// (u - 0.5) with u the plane's RAN2 draws in (j, i) order over the interior cells.
+__global__ void ic_perturb_kernel(double* plane, const double* u, int64_t nx, int64_t ny, double ampt) {
+    const int64_t npx = nx - 2, n = npx * (ny - 2);
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = 1 + c % npx, j = 1 + c / npx;
+        const double w = 1.0 + ampt * (u[c] - 0.5);
+        plane[j * nx + i] *= w;
+    }
+}
+
+// Periodic x/y ghost cells of every plane from the interior (the result of the host's row-then-
+// column ghost copy, src/communicate.cpp:70-168 on one domain).
+__global__ void ic_ghost_kernel(double* f, int64_t nx, int64_t ny, int64_t nz) {
+    const int64_t ring = 2 * nx + 2 * (ny - 2), n = ring * nz;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = c / ring, r = c % ring;
+        int64_t i, j;
+        if (r < nx) { i = r; j = 0; }
+        else if (r < 2 * nx) { i = r - nx; j = ny - 1; }
+        else if (r < 2 * nx + (ny - 2)) { i = 0; j = 1 + (r - 2 * nx); }
+        else { i = nx - 1; j = 1 + (r - 2 * nx - (ny - 2)); }
+        const int64_t si = i == 0 ? nx - 2 : (i == nx - 1 ? 1 : i);
+        const int64_t sj = j == 0 ? ny - 2 : (j == ny - 1 ? 1 : j);
+        f[(k * ny + j) * nx + i] = f[(k * ny + sj) * nx + si];
     }
 }
 
@@ -820,6 +875,113 @@ int r3d_gpu_destroy(r3d_gpu* g) {
     return R3D_OK;
 }
 
+namespace r3dg {
+
+// Device memory freed when it goes out of scope (after the handle's stream has drained).
+struct DeviceBuffer {
+    void* p = nullptr;
+    cudaStream_t st = nullptr;
+    explicit DeviceBuffer(size_t bytes, cudaStream_t s = nullptr) : st(s) { cuda_ok(cudaMalloc(&p, bytes), "cudaMalloc"); }
+    ~DeviceBuffer() {
+        if (st) cudaStreamSynchronize(st);
+        cudaFree(p);
+    }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+};
+
+// The seeded temperature perturbation of the initial condition into t (the handle's planes in
+// the reference layout, on the device), then its periodic x/y ghosts.  The RAN2 stream is one
+// sequential chain (a shuffle table indexed by the previous draw), so the host draws it plane by
+// plane into a ring of pinned buffers while the device copies and applies the planes before.
+void perturb_temperature(r3d_gpu* g, double* t) {
+    const r3d_params& p = g->p;
+    const Derived& d = g->d;
+    const int64_t NX = d.nx, NY = d.ny, NZ = d.nz, per = (int64_t)p.npx * p.npy;
+    PerturbationDraws draws(p, g->z0, g->nloc);
+    constexpr int kRing = 4;
+    if (draws.last() >= draws.first()) {
+        double* host = nullptr;
+        cuda_ok(cudaMallocHost(&host, kRing * per * sizeof(double)), "cudaMallocHost(draws)");
+        struct FreeHost {
+            double* p;
+            ~FreeHost() { cudaFreeHost(p); }
+        } free_host{host};
+        DeviceBuffer dev(kRing * per * sizeof(double), g->stream);
+        cudaEvent_t ev[kRing] = {};
+        struct Events {
+            cudaEvent_t* e;
+            ~Events() {
+                for (int s = 0; s < kRing; ++s)
+                    if (e[s]) cudaEventDestroy(e[s]);
+            }
+        } events{ev};
+        for (int s = 0; s < kRing; ++s) cuda_ok(cudaEventCreateWithFlags(&ev[s], cudaEventDisableTiming), "event");
+        const unsigned blocks = (unsigned)std::min<int64_t>((per + 255) / 256, (int64_t)g->num_sms * 8);
+        for (int64_t k = draws.first(), n = 0; k <= draws.last(); ++k, ++n) {
+            const int s = (int)(n % kRing);
+            double* h = host + s * per;
+            double* u = static_cast<double*>(dev.p) + s * per;
+            if (n >= kRing) cuda_ok(cudaEventSynchronize(ev[s]), "draw ring");  // plane n - kRing is done
+            draws.next_plane(h);
+            cuda_ok(cudaMemcpyAsync(u, h, per * sizeof(double), cudaMemcpyHostToDevice, g->stream), "draws");
+            ic_perturb_kernel<<<blocks, 256, 0, g->stream>>>(t + k * NX * NY, u, NX, NY, p.ampt);
+            cuda_ok(cudaGetLastError(), "ic_perturb_kernel");
+            cuda_ok(cudaEventRecord(ev[s], g->stream), "event");
+        }
+        cuda_ok(cudaStreamSynchronize(g->stream), "draws");
+    }
+    const int64_t ring = (2 * NX + 2 * (NY - 2)) * NZ;
+    ic_ghost_kernel<<<(unsigned)std::min<int64_t>((ring + 255) / 256, (int64_t)g->num_sms * 8), 256, 0, g->stream>>>(
+        t, NX, NY, NZ);
+    cuda_ok(cudaGetLastError(), "ic_ghost_kernel");
+}
+
+// Puts field q, given on the device in the reference layout (contiguous nx*ny*nz FP64, the
+// handle's planes), into both state buffers in the handle's own form.
+void place_field(r3d_gpu* g, int q, const double* src, const Fp64Staging* stg) {
+    const Derived& d = g->d;
+    if (g->fp32) {
+        to_fp32_kernel<<<stg->blocks(), 256, 0, g->stream>>>(g->X32[0][q], g->geo.pitch, g->geo.plane, src, d.nx,
+                                                             d.ny, d.nz, stg->bg(q));
+        cuda_ok(cudaGetLastError(), "state32");
+        // the second buffer gets the same contents on the device (its z ghost planes are never
+        // written by a stage)
+        cuda_ok(cudaMemcpyAsync(g->X32[1][q], g->X32[0][q], (size_t)g->geo.plane * d.nz * sizeof(float),
+                                cudaMemcpyDeviceToDevice, g->stream),
+                "state32");
+    } else {
+        cuda_ok(cudaMemcpy2DAsync(g->X[0][q], g->geo.pitch * sizeof(double), src, d.nx * sizeof(double),
+                                  d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyDeviceToDevice, g->stream),
+                "state");
+        cuda_ok(cudaMemcpyAsync(g->X[1][q], g->X[0][q], (size_t)g->geo.plane * d.nz * sizeof(double),
+                                cudaMemcpyDeviceToDevice, g->stream),
+                "state");
+    }
+}
+
+// The scalars, the dt reduction's start and the dt limits of the new state (end of an upload).
+void finish_state(r3d_gpu* g, const r3d_scalars* sc) {
+    g->cur = 0;
+    r3dk::Scalars h{};
+    h.dt = sc->dt; h.timc = sc->timc; h.timt = sc->timt; h.timi = sc->timi;
+    h.umach = sc->umach; h.tb = sc->tb; h.nit = sc->nit;
+    h.thr_on = g->dt_filter ? 1 : 0;
+    h.thr_local = (g->z0 != 0 || g->nloc != g->p.npz) ? 1 : 0;
+    h.thr_margin = g->thr_margin;
+    *g->hsc = h;
+    cuda_ok(cudaMemcpyAsync(g->dsc, g->hsc, sizeof(h), cudaMemcpyHostToDevice, g->stream), "upload scalars");
+    g->bnd.tb = sc->tb;
+    g->host_timc = sc->timc;
+    g->host_timi = sc->timi;
+    cuda_ok(r3dk::launch_reset_reduction(g->dsc, g->stream), "reset");
+    launch_dt_full_any(g);
+    cuda_ok(cudaStreamSynchronize(g->stream), "upload");
+    g->uploaded = true;
+}
+
+}  // namespace r3dg
+
 int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) {
     return guarded([&] {
         if (!g || !st || !sc) throw std::invalid_argument("null argument");
@@ -834,57 +996,81 @@ int r3d_gpu_upload(r3d_gpu* g, const r3d_host_state* st, const r3d_scalars* sc) 
         for (auto l : lines)
             if (!l) throw std::invalid_argument("r3d_host_state metric line is NULL");
         upload_lines(g, st);
+        const size_t n = (size_t)d.nx * d.ny * d.nz;
         if (g->fp32) {
             upload_background(g, st);
             // each field: one contiguous FP64 copy into a staging buffer, then the deviation from
             // the background and the rounding to FP32 on the device
             Fp64Staging stg(g);
             for (int q = 0; q < 5; ++q) {
-                cuda_ok(cudaMemcpyAsync(stg.buf, src[q], stg.n * sizeof(double), cudaMemcpyHostToDevice, g->stream),
+                cuda_ok(cudaMemcpyAsync(stg.buf, src[q], n * sizeof(double), cudaMemcpyHostToDevice, g->stream),
                         "upload state32");
-                to_fp32_kernel<<<stg.blocks(), 256, 0, g->stream>>>(g->X32[0][q], g->geo.pitch, g->geo.plane, stg.buf,
-                                                                    d.nx, d.ny, d.nz, stg.bg(q));
-                cuda_ok(cudaGetLastError(), "upload state32");
-                // the second buffer gets the same contents on the device (its z ghost planes are
-                // never written by a stage)
-                cuda_ok(cudaMemcpyAsync(g->X32[1][q], g->X32[0][q], (size_t)g->geo.plane * d.nz * sizeof(float),
-                                        cudaMemcpyDeviceToDevice, g->stream),
-                        "upload state32");
+                place_field(g, q, stg.buf, &stg);
             }
         } else {
             for (int q = 0; q < g->nfields; ++q) {
                 // one contiguous host-to-device copy into the accumulator (dead between steps:
                 // the first stage rewrites it), then the re-pitch on the device - a pitched
                 // host-to-device copy runs at about half the link rate
-                const size_t n = (size_t)d.nx * d.ny * d.nz;
                 cuda_ok(cudaMemcpyAsync(g->Z[q], src[q], n * sizeof(double), cudaMemcpyHostToDevice, g->stream),
                         "upload state");
-                cuda_ok(cudaMemcpy2DAsync(g->X[0][q], g->geo.pitch * sizeof(double), g->Z[q], d.nx * sizeof(double),
-                                          d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyDeviceToDevice, g->stream),
-                        "upload state");
-                // the second buffer gets the same contents on the device (its z ghost planes are
-                // never written by a stage)
-                cuda_ok(cudaMemcpyAsync(g->X[1][q], g->X[0][q], (size_t)g->geo.plane * d.nz * sizeof(double),
-                                        cudaMemcpyDeviceToDevice, g->stream),
-                        "upload state");
+                place_field(g, q, g->Z[q], nullptr);
             }
         }
-        g->cur = 0;
-        r3dk::Scalars h{};
-        h.dt = sc->dt; h.timc = sc->timc; h.timt = sc->timt; h.timi = sc->timi;
-        h.umach = sc->umach; h.tb = sc->tb; h.nit = sc->nit;
-        h.thr_on = g->dt_filter ? 1 : 0;
-        h.thr_local = (g->z0 != 0 || g->nloc != g->p.npz) ? 1 : 0;
-        h.thr_margin = g->thr_margin;
-        *g->hsc = h;
-        cuda_ok(cudaMemcpyAsync(g->dsc, g->hsc, sizeof(h), cudaMemcpyHostToDevice, g->stream), "upload scalars");
-        g->bnd.tb = sc->tb;
-        g->host_timc = sc->timc;
-        g->host_timi = sc->timi;
-        cuda_ok(r3dk::launch_reset_reduction(g->dsc, g->stream), "reset");
-        launch_dt_full_any(g);
-        cuda_ok(cudaStreamSynchronize(g->stream), "upload");
-        g->uploaded = true;
+        finish_state(g, sc);
+    });
+}
+
+int r3d_gpu_setup(r3d_gpu* g, r3d_scalars* sc) {
+    return guarded([&] {
+        if (!g || !sc) throw std::invalid_argument("null argument");
+        DeviceGuard dg(g->device);
+        Range r("r3d.setup");
+        const r3d_params& p = g->p;
+        const Derived& d = g->d;
+        const int64_t NX = d.nx, NY = d.ny, NZ = d.nz;
+        // metric lines and background columns on the host (1D), then uploaded as by r3d_gpu_upload
+        std::vector<double> lines[14];
+        const int64_t len[14] = {NX, NX, NX, NX, NY, NY, NY, NY, NZ, NZ, NZ, NZ, NZ, NZ};
+        for (int q = 0; q < 14; ++q) lines[q].assign((size_t)len[q], 0.0);
+        r3d_host_state st{};
+        double** lp[14] = {&st.exx, &st.dxxdx, &st.d2xxdx2, &st.ddx, &st.wyy, &st.dyydy, &st.d2yydy2,
+                           &st.ddy, &st.zee, &st.dzzdz, &st.d2zzdz2, &st.ddz, &st.rkapa, &st.dkapa};
+        for (int q = 0; q < 14; ++q) *lp[q] = lines[q].data();
+        setup_lines(p, st, g->z0, g->nloc);
+        upload_lines(g, &st);
+        std::unique_ptr<Fp64Staging> stg;
+        if (g->fp32) {
+            upload_background(g, &st);
+            stg.reset(new Fp64Staging(g));
+        }
+        const IcColumns c = ic_columns(p, g->z0, g->nloc);
+        DeviceBuffer cols(3 * (size_t)NZ * sizeof(double));
+        double* dcol = static_cast<double*>(cols.p);
+        std::vector<double> hc(c.t);
+        hc.insert(hc.end(), c.r.begin(), c.r.end());
+        hc.insert(hc.end(), c.bfac.begin(), c.bfac.end());
+        cuda_ok(cudaMemcpyAsync(dcol, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, g->stream),
+                "setup columns");
+        const size_t n = (size_t)NX * NY * NZ;
+        const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)g->num_sms * 16);
+        // fields in the order the temperature needs its draws last: momenta, density, B, then T
+        const int order[8] = {0, 1, 2, 3, 5, 6, 7, 4};
+        for (int oi = 0; oi < 8; ++oi) {
+            const int q = order[oi];
+            if (q >= g->nfields) continue;
+            double* buf = g->fp32 ? stg->buf : g->Z[q];
+            const int kind = q == 4 ? 1 : (q == 3 ? 2 : (q == 5 ? 3 : 0));
+            ic_field_kernel<<<blocks, 256, 0, g->stream>>>(buf, NX, NY, NZ, kind, dcol, dcol + NZ, dcol + 2 * NZ,
+                                                          d.obeta, p.lmag, g->z0, (int64_t)p.npz + 2);
+            cuda_ok(cudaGetLastError(), "ic_field_kernel");
+            if (q == 4) perturb_temperature(g, buf);
+            place_field(g, q, buf, stg.get());
+        }
+        r3d_scalars s{};
+        s.tb = c.tb;
+        finish_state(g, &s);
+        *sc = s;
     });
 }
 

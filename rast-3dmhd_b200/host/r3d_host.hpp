@@ -61,6 +61,34 @@ class Ran2 {
 // Static polytrope by Bulirsch-Stoer integration, T(k), R(k) for k = 0..npz-1.
 void static_profile(const r3d_params& p, std::vector<double>& t, std::vector<double>& r);
 
+// The parts of the initial condition (src/static_ic.cpp:24-161) on global planes z0 .. z0+nz+1
+// (the whole domain: z0 = 0, nz = npz), local plane k = global plane z0+k:
+//  * columns: t[k], r[k] the static T and rho of the plane (interior cells; ghost planes: the
+//    top T(0), R(0) and the bottom tb, rb), bfac[k] the magnetic layer's Bx (0 without LMAG and
+//    on the ghost planes), tb;
+//  * the metric lines into st's line arrays (x/y whole, z from global index z0, nz+2 entries);
+//  * the perturbation draws: the RAN2 stream in the reference's global (k, j, i) order, one
+//    interior plane at a time (a slab skips the draws of the planes above it).
+struct IcColumns {
+    std::vector<double> t, r, bfac;
+    double tb = 1.0, rb = 1.0;
+};
+IcColumns ic_columns(const r3d_params& p, int z0, int nz);
+void setup_lines(const r3d_params& p, const r3d_host_state& st, int z0, int nz);
+class PerturbationDraws {
+   public:
+    PerturbationDraws(const r3d_params& p, int z0, int nz);
+    // local planes [first, last] that carry the perturbation (empty when ampt == 0)
+    int64_t first() const { return first_; }
+    int64_t last() const { return last_; }
+    // the npx*npy draws of the next plane, (j, i) order, into out
+    void next_plane(double* out);
+
+   private:
+    Ran2 rng_;
+    int64_t per_plane_, first_, last_;
+};
+
 // Fill st (arrays sized by the caller) with metrics, conductivity, the static IC, the seeded
 // temperature perturbation and the periodic ghosts; returns tb in sc.
 void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc, int z0, int nz);

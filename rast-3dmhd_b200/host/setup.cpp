@@ -320,19 +320,42 @@ void fill_ghosts(double* f, int64_t nx, int64_t ny, int64_t nz) {
     }
 }
 
-// The initial state on global planes z0 .. z0+nz+1 (the whole domain: z0 = 0, nz = npz); the z
-// metric lines are written from global index z0 on, nz+2 entries.
-void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc, int z0, int nz) {
-    check_params(p);
+IcColumns ic_columns(const r3d_params& p, int z0, int nz) {
     if (z0 < 0 || nz < 1 || z0 + nz > p.npz) throw std::invalid_argument("z range outside the domain");
     const Derived d = derive(p);
-    const int64_t NX = d.nx, NY = d.ny, NZ = (int64_t)nz + 2, N = NX * NY * NZ;
-    const int64_t NZG = d.nz;  // global planes (with the two ghost planes)
-    auto need = [](const double* a, const char* n) {
-        if (!a) throw std::invalid_argument(std::string("r3d_host_state.") + n + " is NULL");
-    };
-    need(st.ru, "ru"); need(st.rv, "rv"); need(st.rw, "rw"); need(st.ro, "ro"); need(st.tt, "tt");
-    if (p.lmag) { need(st.bx, "bx"); need(st.by, "by"); need(st.bz, "bz"); }
+    const int64_t NZ = (int64_t)nz + 2, NZG = d.nz;
+    IcColumns c;
+    std::vector<double> T, R;
+    static_profile(p, T, R);
+    c.tb = T[p.npz - 1];
+    c.rb = R[p.npz - 1];
+    c.t.assign(NZ, 0.0);
+    c.r.assign(NZ, 0.0);
+    c.bfac.assign(NZ, 0.0);
+    // src/static_ic.cpp:53-89 stitched over the ranks: ghost top = T(0), interior k = T(k-1),
+    // ghost bottom = tb
+    for (int64_t k = 0; k < NZ; ++k) {
+        const int64_t kg = z0 + k;
+        c.t[k] = kg == 0 ? T[0] : (kg == NZG - 1 ? c.tb : T[kg - 1]);
+        c.r[k] = kg == 0 ? R[0] : (kg == NZG - 1 ? c.rb : R[kg - 1]);
+    }
+    if (p.lmag) {
+        // magnetic layer (src/static_ic.cpp:94-108)
+        const Metrics m = build_metrics(p, d);
+        const double cln = widen(-4.0f * logf(2.0f)) / (p.bfh * p.bfh);
+        for (int64_t k = 0; k < NZ; ++k) {
+            const int64_t kg = z0 + k;
+            if (kg < 1 || kg > NZG - 2) continue;
+            const double z = m.z.s[kg];
+            c.bfac[k] = p.ampb * std::exp(cln * (z - p.bzp) * (z - p.bzp));
+        }
+    }
+    return c;
+}
+
+void setup_lines(const r3d_params& p, const r3d_host_state& st, int z0, int nz) {
+    const Derived d = derive(p);
+    const int64_t NZ = (int64_t)nz + 2;
     const Metrics m = build_metrics(p, d);
     auto put = [](double* dst, const std::vector<double>& v) {
         if (dst) std::memcpy(dst, v.data(), sizeof(double) * v.size());
@@ -344,6 +367,37 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc,
     };
     putz(st.zee, m.z.s); putz(st.dzzdz, m.z.d1); putz(st.d2zzdz2, m.z.d2); putz(st.ddz, m.z.dd);
     putz(st.rkapa, m.rkapa); putz(st.dkapa, m.dkapa);
+}
+
+// temperature perturbation draws (src/static_ic.cpp:114-159): global (k, j, i) order over the
+// interior planes 1 .. npz; a slab skips the draws of the interior planes above it
+PerturbationDraws::PerturbationDraws(const r3d_params& p, int z0, int nz)
+    : rng_(-p.seed), per_plane_((int64_t)p.npx * p.npy) {
+    const int64_t NZG = (int64_t)p.npz + 2, NZ = (int64_t)nz + 2;
+    const int64_t kfirst = std::max<int64_t>(1, z0), klast = std::min<int64_t>(NZG - 2, z0 + NZ - 1);
+    first_ = kfirst - z0;
+    last_ = p.ampt != 0.0 ? klast - z0 : first_ - 1;
+    if (p.ampt != 0.0)
+        for (int64_t n = 0; n < (kfirst - 1) * per_plane_; ++n) rng_.next();
+}
+
+void PerturbationDraws::next_plane(double* out) {
+    for (int64_t n = 0; n < per_plane_; ++n) out[n] = rng_.next();
+}
+
+// The initial state on global planes z0 .. z0+nz+1 (the whole domain: z0 = 0, nz = npz); the z
+// metric lines are written from global index z0 on, nz+2 entries.
+void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc, int z0, int nz) {
+    check_params(p);
+    if (z0 < 0 || nz < 1 || z0 + nz > p.npz) throw std::invalid_argument("z range outside the domain");
+    const Derived d = derive(p);
+    const int64_t NX = d.nx, NY = d.ny, NZ = (int64_t)nz + 2;
+    auto need = [](const double* a, const char* n) {
+        if (!a) throw std::invalid_argument(std::string("r3d_host_state.") + n + " is NULL");
+    };
+    need(st.ru, "ru"); need(st.rv, "rv"); need(st.rw, "rw"); need(st.ro, "ro"); need(st.tt, "tt");
+    if (p.lmag) { need(st.bx, "bx"); need(st.by, "by"); need(st.bz, "bz"); }
+    setup_lines(p, st, z0, nz);
 
     // zero every field plane by plane over the host threads (the first touch of fresh pages
     // is most of the set-up time on large grids)
@@ -352,38 +406,24 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc,
 #pragma omp parallel for schedule(static)
         for (int64_t k = 0; k < NZ; ++k) std::memset(a + k * NX * NY, 0, sizeof(double) * NX * NY);
     }
-    (void)N;
 
-    std::vector<double> T, R;
-    static_profile(p, T, R);
-    const double tb = T[p.npz - 1], rb = R[p.npz - 1];
+    const IcColumns c = ic_columns(p, z0, nz);
     auto at = [&](int64_t i, int64_t j, int64_t k) { return i + NX * (j + NY * k); };
-    // columns (src/static_ic.cpp:53-89): ghost top = T(0), interior k = T(k-1), ghost bottom = tb
 #pragma omp parallel for schedule(static)
-    for (int64_t k = 0; k < NZ; ++k) {
-        const int64_t kg = z0 + k;
-        const double tv = kg == 0 ? T[0] : (kg == NZG - 1 ? tb : T[kg - 1]);
-        const double rv = kg == 0 ? R[0] : (kg == NZG - 1 ? rb : R[kg - 1]);
+    for (int64_t k = 0; k < NZ; ++k)
         for (int64_t j = 1; j <= NY - 2; ++j)
             for (int64_t i = 1; i <= NX - 2; ++i) {
-                st.tt[at(i, j, k)] = tv;
-                st.ro[at(i, j, k)] = rv;
+                st.tt[at(i, j, k)] = c.t[k];
+                st.ro[at(i, j, k)] = c.r[k];
             }
-    }
     if (p.lmag) {
-        // magnetic layer (src/static_ic.cpp:94-108)
-        const double cln = widen(-4.0f * logf(2.0f)) / (p.bfh * p.bfh);
-        for (int64_t k = 0; k < NZ; ++k) {
-            const int64_t kg = z0 + k;
-            if (kg < 1 || kg > NZG - 2) continue;
-            const double z = m.z.s[kg];
-            const double bfac = p.ampb * std::exp(cln * (z - p.bzp) * (z - p.bzp));
-            for (int64_t n = at(0, 0, k); n < at(0, 0, k + 1); ++n) st.bx[n] = bfac;
-        }
+        // magnetic layer (src/static_ic.cpp:94-108): Bx over whole interior planes, and the
+        // density correction with the unperturbed T
 #pragma omp parallel for schedule(static)
         for (int64_t k = 0; k < NZ; ++k) {
             const int64_t kg = z0 + k;
-            if (kg < 1 || kg > NZG - 2) continue;
+            if (kg < 1 || kg > d.nz - 2) continue;
+            for (int64_t n = at(0, 0, k); n < at(0, 0, k + 1); ++n) st.bx[n] = c.bfac[k];
             for (int64_t j = 1; j <= NY - 2; ++j)
                 for (int64_t i = 1; i <= NX - 2; ++i) {
                     const int64_t n = at(i, j, k);
@@ -391,20 +431,16 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc,
                 }
         }
     }
-    if (p.ampt != 0.0) {
-        // temperature perturbation (src/static_ic.cpp:114-159), global (k, j, i) draw order
-        // a slab skips the draws of the interior planes above it
-        Ran2 rng(-p.seed);
-        const int64_t kfirst = std::max<int64_t>(1, z0), klast = std::min<int64_t>(NZG - 2, z0 + NZ - 1);
-        for (int64_t n = 0; n < (kfirst - 1) * (NX - 2) * (NY - 2); ++n) rng.next();
-        for (int64_t kg = kfirst; kg <= klast; ++kg) {
-            const int64_t k = kg - z0;
-            for (int64_t j = 1; j <= NY - 2; ++j)
-                for (int64_t i = 1; i <= NX - 2; ++i) {
-                    const double w = 1.0 + p.ampt * (rng.next() - 0.5);
-                    st.tt[at(i, j, k)] *= w;
-                }
-        }
+    PerturbationDraws draws(p, z0, nz);
+    std::vector<double> plane((size_t)p.npx * p.npy);
+    for (int64_t k = draws.first(); k <= draws.last(); ++k) {
+        draws.next_plane(plane.data());
+        const double* u = plane.data();
+        for (int64_t j = 1; j <= NY - 2; ++j)
+            for (int64_t i = 1; i <= NX - 2; ++i) {
+                const double w = 1.0 + p.ampt * (*u++ - 0.5);
+                st.tt[at(i, j, k)] *= w;
+            }
     }
     for (double* a : {st.ru, st.rv, st.rw, st.tt, st.ro}) fill_ghosts(a, NX, NY, NZ);
     if (p.lmag)
@@ -414,7 +450,7 @@ void setup_state(const r3d_params& p, const r3d_host_state& st, r3d_scalars& sc,
     sc.timt = 0.0;
     sc.timi = 0.0;
     sc.umach = 0.0;
-    sc.tb = tb;
+    sc.tb = c.tb;
     sc.nit = 0;
 }
 

@@ -110,6 +110,8 @@ def lib():
         L.r3d_gpu_run_timed.argtypes = [vp, ip, ctypes.POINTER(Scalars), ctypes.POINTER(Timing)]
         L.r3d_gpu_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.r3d_gpu_compare.argtypes = [vp, vp, ctypes.c_void_p]
+        L.r3d_gpu_setup.argtypes = [vp, ctypes.POINTER(Scalars)]
+        L.r3d_gpu_download_accumulators.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
         L.r3d_gpu_debug_tma_extra.argtypes = [vp, ctypes.c_uint]
         L.r3d_gpu_debug_dt_filter.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         L.r3d_gpu_fluxes.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
@@ -330,6 +332,24 @@ class GpuSim:
         m, e = ctypes.c_double(), ctypes.c_double()
         _check(lib().r3d_gpu_totals(self.h, ctypes.byref(m), ctypes.byref(e)))
         return m.value, e.value
+
+    def setup(self) -> Dict[str, float]:
+        """Build the initial state on the device (r3d_gpu_setup): the same state as
+        upload(HostState.setup(p)), without host 3D arrays; returns the scalars."""
+        sc = Scalars()
+        _check(lib().r3d_gpu_setup(self.h, ctypes.byref(sc)))
+        return sc.as_dict()
+
+    def accumulators(self) -> Dict[str, np.ndarray]:
+        """The RK accumulators zru .. ztt (+ zbx zby zbz), shapes (NZ, NY, NX), interior cells."""
+        NX, NY, NZ = dims(self.p)
+        if self.slab is not None:
+            NZ = self.slab[1] + 2
+        names = ["zru", "zrv", "zrw", "zro", "ztt"] + (["zbx", "zby", "zbz"] if self.p.lmag else [])
+        out = {n: np.zeros((NZ, NY, NX)) for n in names}
+        ptrs = (ctypes.c_void_p * 8)(*([out[n].ctypes.data for n in names] + [None] * (8 - len(names))))
+        _check(lib().r3d_gpu_download_accumulators(self.h, ptrs))
+        return out
 
     def compare(self, ref: "GpuSim") -> Dict[str, Dict[str, float]]:
         """Error of this state against ref's, on the device: per field rel_l2 =

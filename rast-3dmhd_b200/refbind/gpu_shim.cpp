@@ -191,7 +191,8 @@ void block_global(const Derived& d, int mypey, int mypez, HostBlock& blk, HostBl
         }
     }
     if (!gather) return;
-    for (int q = 0; q < 4; ++q) glob.lx[q] = blk.lx[q];  // x is not decomposed
+    if (mypey == 0 && mypez == 0)  // x is not decomposed: rank 0's lines (other blocks carry none)
+        for (int q = 0; q < 4; ++q) glob.lx[q] = blk.lx[q];
     if (mypez == 0)
         for (int jl = 0; jl < ny; ++jl) {
             const bool jin = (jl >= 1 && jl <= d.nry) || (jl == 0 && mypey == 0) ||
