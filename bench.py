@@ -291,19 +291,19 @@ def fp32_error_run(R, local, grid, steps, flags=(), seed=None):
     out = {"grid": list(grid), "steps": steps, "seed": seed, "flags": list(flags)}
     p64 = R.parse(base + ["--precision", "fp64"])
     p32 = R.parse(base + ["--precision", "fp32bulk"])
-    st = R.HostState.setup(p64)  # one host initial state for both forms
-    totals, times = {}, {}
+    totals, times, setup_s = {}, {}, {}
     with R.GpuSim(p64) as s64, R.GpuSim(p32) as s32:
         for prec, sim in (("fp64", s64), ("fp32bulk", s32)):
-            sim.upload(st)
+            t0 = time.perf_counter()
+            sim.setup()  # the same initial state for both forms, built on the device
+            setup_s[prec] = time.perf_counter() - t0
             m0, e0 = sim.totals()
             _, tm = sim.run_timed(steps)
             m1, e1 = sim.totals()
             totals[prec] = {"mass_drift": (m1 - m0) / m0, "energy_drift": (e1 - e0) / e0}
             times[prec] = tm["total_ms"] / steps
-        del st
         err = s32.compare(s64)
-    out.update({"error": err, "max_rel_l2": max(v["rel_l2"] for v in err.values()),
+    out.update({"device_setup_s": setup_s, "error": err, "max_rel_l2": max(v["rel_l2"] for v in err.values()),
                 "totals": totals, "ms_per_step": times, "speedup": times["fp64"] / times["fp32bulk"],
                 "mcell_updates_per_s": {k: grid[0] * grid[1] * grid[2] / (v / 1e3) / 1e6 for k, v in times.items()}})
     return out
@@ -496,7 +496,9 @@ def main():
     if world == 1 and not args.slabs:
         p = R.parse(FLAGS + mag + ["--seed", str(SEED), "--gpu", str(local), "--precision", args.precision])
         cells = GRID[0] * GRID[1] * GRID[2]
+        t_setup = time.perf_counter()
         st = R.HostState.setup(p)
+        t_setup = time.perf_counter() - t_setup
         sim = R.GpuSim(p)
     else:
         # weak scaling: the domain is npx x npy x (npz * N), one z slab of npz planes per GPU,
@@ -507,10 +509,14 @@ def main():
                      "--seed", str(SEED), "--gpu", str(local), "--precision", args.precision] + mag)
         z0, nz = D.slab_of(p.npz, rank, world)
         cells = GRID[0] * GRID[1] * nz
+        t_setup = time.perf_counter()
         st = R.HostState.setup_slab(p, z0, nz)
+        t_setup = time.perf_counter() - t_setup
         sim = R.GpuSim(p, slab=(z0, nz))
         sim.halo_init(D.share_unique_id(rank, pg), rank, world)
+    t_upload = time.perf_counter()
     sim.upload(st)
+    t_upload = time.perf_counter() - t_upload
     with ClockSampler(local) as clk:
         sim.run(args.warmup)                     # untimed warm-up
         clk.wait_first()
@@ -558,8 +564,14 @@ def main():
                 "kernel": ("stage_fp32" if fp32 else "stage_fp64") + " (fused FLUXES + RK3 stage update)",
                 "step_frac": (cells * bytes_step / (ms_per_step / 1e3) / 1e9) / peak}
 
+    # the same initial state built on the device (r3d_gpu_setup), for the set-up time
+    t_dev = time.perf_counter()
+    sim.setup()
+    t_dev = time.perf_counter() - t_dev
     sim.close()
-    extra = {}
+    extra = {"setup": {"host_setup_s": t_setup, "upload_s": t_upload, "device_setup_s": t_dev,
+                       "note": "initial state of the headline grid: host set-up (arrays on the host) + "
+                               "upload, against r3d_gpu_setup (no host 3D arrays); wall clock"}}
     if not args.no_extra and not args.grid and not fp32 and world == 1 and not args.slabs and not args.mhd:
         extra["fp32bulk_504x504x512"] = side_run(R, FLAGS + ["--seed", str(SEED), "--precision", "fp32bulk",
                                                              "--gpu", str(local)], args.steps, args.warmup,

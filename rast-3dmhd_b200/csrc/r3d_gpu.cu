@@ -241,7 +241,7 @@ int stage_chunk_depth(const r3d_params& p, bool fp32, int tile_rows, int nloc, i
     if (fp32) r3dk::stage_fp32_box(&tbx, &tby);
     else r3dk::stage_fp64_box(tile_rows, &tbx, &tby);
     const int64_t tiles = (int64_t)((p.npx + 31) / 32) * ((p.npy + (int)tby - 3) / ((int)tby - 2));
-    const int64_t slots = (int64_t)num_sms * ((fp32 ? 3 : 2) - (p.lmag && tby == 10 ? 1 : 0));
+    const int64_t slots = (int64_t)num_sms * (fp32 ? r3dk::stage_fp32_ctas_per_sm() : 2 - (p.lmag && tby == 10 ? 1 : 0));
     if (p.lmag && tby == 8) {
         // 32x6 MHD tiles, two CTAs per SM: 12-plane chunks.  Measured on B200 against the
         // earlier 16/32-plane choice: 126x126x256 0.962 -> 0.922 ms per step, 252x252x256
@@ -392,7 +392,7 @@ void enqueue_stage(r3d_gpu* g, int s) {
     Range r("r3d.stage");
     if (g->fp32) {
         r3dk::FieldSet32 fs = fieldset32(g);
-        cuda_ok(r3dk::launch_stage_fp32(s, g->maps[g->cur], g->zmaps, g->geo, g->ph, g->lines, g->bg, fs, g->dsc,
+        cuda_ok(r3dk::launch_stage_fp32(s, g->maps[g->cur], g->geo, g->ph, g->lines, g->bg, fs, g->dsc,
                                         g->kchunk, g->stream),
                 "stage32");
         cuda_ok(r3dk::launch_bcon_fp32(g->geo, g->ph, g->lines, g->bnd, g->bg, fs, g->dsc, s == 2 ? 1 : 0, g->stream),
@@ -428,7 +428,7 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
         tm.begin();
         if (g->fp32) {
             r3dk::FieldSet32 fs = fieldset32(g);
-            cuda_ok(r3dk::launch_stage_fp32(s, g->maps[g->cur], g->zmaps, g->geo, g->ph, g->lines, g->bg, fs, g->dsc, g->kchunk, g->stream), "stage32");
+            cuda_ok(r3dk::launch_stage_fp32(s, g->maps[g->cur], g->geo, g->ph, g->lines, g->bg, fs, g->dsc, g->kchunk, g->stream), "stage32");
             tm.end(0);
             tm.begin();
             cuda_ok(r3dk::launch_bcon_fp32(g->geo, g->ph, g->lines, g->bnd, g->bg, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon32");
@@ -769,10 +769,6 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
                     for (int q = 0; q < 5; ++q)
                         g->maps[b].m[q] = field_map(g->X32[b][q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
                                                     bx, by, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float));
-                r3dk::stage_fp32_zbox(&bx, &by);
-                for (int q = 0; q < 5; ++q)  // Z rows start at interior column 1
-                    g->zmaps.m[q] = field_map(g->Z32[q], d.nx, d.ny, d.nz, g->geo.pitch, g->geo.plane,
-                                              bx, by, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float));
             } else {
                 const size_t nbytes = (size_t)g->geo.plane * d.nz * sizeof(double);
                 for (int b = 0; b < 2; ++b)

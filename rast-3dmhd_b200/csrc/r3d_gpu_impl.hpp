@@ -35,12 +35,10 @@ struct r3d_gpu {
     int nfields = 5;
     double* X[2][r3dk::kMaxFields] = {};
     r3dk::StageMaps maps[2];  // TMA maps of X[0] and X[1] (ru rv rw ro tt)
-    r3dk::StageMaps zmaps;    // TMA maps of the FP32 accumulators Z32
     double* Z[r3dk::kMaxFields] = {};
     // FP32-bulk state (precision == R3D_PREC_FP32BULK): momenta and rho', T' deviations
     bool fp32 = false;
-    float* X32[2][5] = {};     // element (0,0,0) of each FP32 state array
-    float* X32mem[2][5] = {};  // the allocations (X32 = X32mem + 1)
+    float* X32[2][5] = {};
     float* Z32[5] = {};
     r3dk::Background bg{};
     void* bg_buf = nullptr;

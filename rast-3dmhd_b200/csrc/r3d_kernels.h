@@ -43,13 +43,11 @@ struct Background {
 };
 
 void stage_fp32_box(unsigned* bx, unsigned* by);
-// Z box of the FP32 stage kernel: Z is stored one column left-shifted (element (i,j,k) at
-// k*plane + j*pitch + i-1) so an interior tile starts on a 16-byte boundary.
-void stage_fp32_zbox(unsigned* bx, unsigned* by);
-cudaError_t launch_stage_fp32(int stage, const StageMaps& maps, const StageMaps& zmaps,
-                              const Geometry& g, const Physics& ph, const Lines& L,
-                              const Background& bg, const FieldSet32& fs, Scalars* sc, int kchunk,
-                              cudaStream_t st);
+// CTAs of the FP32-bulk stage kernel resident per SM (the chunk planner's slots).
+int stage_fp32_ctas_per_sm();
+cudaError_t launch_stage_fp32(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
+                              const Lines& L, const Background& bg, const FieldSet32& fs, Scalars* sc,
+                              int kchunk, cudaStream_t st);
 cudaError_t launch_bcon_fp32(const Geometry& g, const Physics& ph, const Lines& L, const Boundary& b,
                              const Background& bg, const FieldSet32& fs, Scalars* sc, int with_dt,
                              cudaStream_t st);

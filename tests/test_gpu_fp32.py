@@ -108,24 +108,23 @@ def test_device_compare_equals_host_norms():
 def test_config4_plume_504x504x2048_fp32bulk_vs_fp64():
     """The FP32-bulk benchmark configuration: 504 x 504 x 2048 with the reference's plume top
     boundary (tp 2, itcon 1, Gaussian at xp = yp = 10, zp 0, hh 1; src/bcon.cpp:43-70), seed 11,
-    50 steps, the FP64 form alongside from the same initial state (63 + 32 GB on the device).
+    50 steps, the FP64 form alongside from the same initial state (63 + 32 GB on the device, built
+    there by r3d_gpu_setup).
     Errors are computed on the device; bar as above: rel L2 <= 1e-5, rel Linf <= 1e-4 per field,
     equal drift of mass and energy, and the FP32-bulk step faster."""
     flags = ["--npx", "504", "--npy", "504", "--npz", "2048", "--seed", "11", "--tp", "2", "--tc", "0",
              "--xp", "10", "--yp", "10", "--zp", "0", "--hh", "1"]
     p64, p32 = R.parse(flags), R.parse(flags + ["--precision", "fp32bulk"])
-    st = R.HostState.setup(p64)
     drift, ms = {}, {}
     with R.GpuSim(p64) as a, R.GpuSim(p32) as b:
         for k, sim in (("fp64", a), ("fp32", b)):
-            sim.upload(st)
+            sim.setup()  # the initial state built on the device: no 21 GB host copy
             m0, e0 = sim.totals()
             sc, tm = sim.run_timed(50)
             m1, e1 = sim.totals()
             drift[k] = ((m1 - m0) / m0, (e1 - e0) / e0)
             ms[k] = tm["total_ms"] / 50
             assert sc["nit"] == 50
-        del st
         err = b.compare(a)
     for n in FIELDS:
         assert err[n]["rel_l2"] <= 1e-5, (n, err[n])

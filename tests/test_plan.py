@@ -14,7 +14,7 @@ def grid(npx, npy, npz, *extra):
 
 @pytest.mark.parametrize("flags,want", [
     (grid(504, 504, 512), (62, 8)),                             # short last chunk (8 x 62 + 16)
-    (grid(504, 504, 512, "--precision", "fp32bulk"), (62, 8)),
+    (grid(504, 504, 512, "--precision", "fp32bulk"), (63, 8)),    # four FP32 CTAs per SM
     (grid(504, 504, 2048), (64, 8)),                            # > 64 waves: the tail is negligible
     (grid(504, 504, 64), (16, 8)),
     (grid(32, 32, 64), (4, 8)),                                 # one partial wave: waves x planes
