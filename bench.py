@@ -48,7 +48,7 @@ BYTES_PER_CELL_STEP = 400.0
 BYTES_PER_CELL_STAGE = BYTES_PER_CELL_STEP / 3.0
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "stage_fp64_504x504x64.md")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic_stage_fp64_504x504x124_k62.md")
 
 
 def peak_hbm():
