@@ -9,9 +9,14 @@ SUBROUTINE FLUXES, lines 2146-2651) is read and its statements are executed as w
   non-zero column 6) joined, statement labels taken from columns 1-5;
 * statements: `DO <label> <var>=<lo>,<hi>` nests closed by `<label> CONTINUE`, assignments to
   arrays or scalars, and `IF (MYPEZ.EQ.0) THEN / ELSE IF (MYPEZ.EQ.NPEZ-1) THEN / ENDIF`;
-* expressions: a recursive-descent parser for + - * / (left to right, unary minus), numbers
-  (4.0E00 ...), scalars and array references; integer index and bound expressions use integer
-  division.
+* expressions: a recursive-descent parser for + - * / and ** (left to right, unary minus),
+  numbers, scalars, array references and the intrinsics EXP, LOG, TANH; integer index and bound
+  expressions use integer division.  Literals without a D exponent (4.0E00, 2.0) are default
+  REAL (single precision) as in Fortran: an operation on two of them, or an intrinsic of one,
+  is evaluated in float32 and widened only when it meets a REAL*8 variable (IMPLICIT REAL*8), so
+  -4.0E00*LOG(2.0E00) is the single-precision product; x**2 is x*x;
+* conditions of IF (...) THEN / ELSE / ENDIF: MYPEZ.EQ.0 and MYPEZ.EQ.NPEZ-1 select the faces
+  (see below); other comparisons (.EQ. .NE. .GT. .LT. .GE. .LE.) of scalars are evaluated.
 
 Each DO nest is executed as one whole-array numpy statement over the loop box.  That is exact
 because no statement of the block reads the array it writes at another index (checked at run
@@ -22,12 +27,14 @@ Arrays are the oracle's global (NZ, NY, NX) arrays; Fortran A(I,J,K) is A[K-1, J
 """
 from __future__ import annotations
 
+import math
 import re
 from typing import Dict, List, Tuple
 
 import numpy as np
 
-ARRAYS_1D = {"DXXDX": 2, "D2XXDX2": 2, "DYYDY": 1, "D2YYDY2": 1, "DZZDZ": 0, "D2ZZDZ2": 0}
+ARRAYS_1D = {"DXXDX": 2, "D2XXDX2": 2, "DYYDY": 1, "D2YYDY2": 1, "DZZDZ": 0, "D2ZZDZ2": 0,
+             "EXX": 2, "WYY": 1, "ZEE": 0}
 
 
 def read_block(path: str, first: int = 2146, last: int = 2651) -> List[Tuple[str, str]]:
@@ -47,7 +54,7 @@ def read_block(path: str, first: int = 2146, last: int = 2651) -> List[Tuple[str
 
 
 # --------------------------------------------------------------------- expressions -------
-_TOK = re.compile(r"\s*(?:(\d+\.\d*(?:[EeDd][+-]?\d+)?|\d+(?:[EeDd][+-]?\d+)?)|([A-Z][A-Z0-9_]*)|(\S))")
+_TOK = re.compile(r"\s*(?:(\d+\.\d*(?:[EeDd][+-]?\d+)?|\d+(?:[EeDd][+-]?\d+)?)|([A-Z][A-Z0-9_]*)|(\*\*|\S))")
 
 
 def _tokens(s: str):
@@ -96,10 +103,17 @@ class _Parser:
         return node
 
     def term(self):
-        node = self.factor()
-        while self.peek()[0] == "op" and self.peek()[1] in "*/":
+        node = self.power()
+        while self.peek()[0] == "op" and self.peek()[1] in ("*", "/"):
             op = self.take()[1]
-            node = (op, node, self.factor())
+            node = (op, node, self.power())
+        return node
+
+    def power(self):
+        node = self.factor()
+        if self.peek() == ("op", "**"):
+            self.take()
+            node = ("**", node, self.factor())
         return node
 
     def factor(self):
@@ -134,13 +148,34 @@ def parse(text: str):
 
 
 # ------------------------------------------------------------------------- evaluation -----
+def _libm(f):
+    """An intrinsic evaluated by the C math library element by element (math.* call libm), as a
+    compiled Fortran does; numpy's vectorised exp/log may differ from libm in the last bit."""
+    vec = np.vectorize(f, otypes=[np.float64])
+
+    def call(x):
+        if isinstance(x, np.ndarray):
+            return vec(x)
+        return f(float(x))
+    return call
+
+
+INTRINSICS = {"EXP": _libm(math.exp), "LOG": _libm(math.log), "TANH": _libm(math.tanh)}
+
+
+def _is_r4(v) -> bool:
+    """A default-REAL (single precision) value: a literal, or a result computed from them."""
+    return isinstance(v, np.float32)
+
+
 class Block:
     """The LMAG statements, executable on a dict of arrays and scalars."""
 
-    def __init__(self, path: str, first: int = 2146, last: int = 2651):
+    def __init__(self, path: str, first: int = 2146, last: int = 2651, guard: str = "LMAG"):
         self.stmts = read_block(path, first, last)
-        if not self.stmts or not re.match(r"IF\s*\(\s*LMAG\s*\)\s*THEN", self.stmts[0][1]):
-            raise ValueError("the block must start with IF (LMAG) THEN")
+        if not self.stmts or not re.match(r"IF\s*\(\s*" + re.escape(guard) + r"\s*\)\s*THEN",
+                                          self.stmts[0][1].replace(" ", "")):
+            raise ValueError(f"the block must start with IF ({guard}) THEN")
 
     # integer expressions (bounds, constant indices)
     def _int(self, node, env, loopvar_offsets=None):
@@ -188,11 +223,26 @@ class Block:
     def _value(self, node, env, box):
         kind = node[0]
         if kind == "num":
-            return float(node[1].replace("D", "E").replace("d", "e"))
+            text = node[1]
+            if "D" in text or "d" in text:  # double-precision literal
+                return float(text.replace("D", "E").replace("d", "e"))
+            return np.float32(text)  # default REAL
         if kind == "id":
             return env[node[1]]
         if kind == "neg":
-            return -self._value(node[1], env, box)
+            v = self._value(node[1], env, box)
+            return np.float32(-v) if _is_r4(v) else -v
+        if kind == "ref" and node[1] in INTRINSICS:
+            v = self._value(node[2][0], env, box)
+            f = INTRINSICS[node[1]]
+            # a single-precision argument gives the single-precision result (the double result
+            # rounded once: the correctly rounded float of these intrinsics)
+            return np.float32(f(v)) if _is_r4(v) else f(v)
+        if kind == "**":
+            base, ex = self._value(node[1], env, box), node[2]
+            if ex[0] != "num" or ex[1] != "2":
+                raise ValueError("only x**2 is supported")
+            return base * base
         if kind == "ref":
             name, args = node[1], node[2]
             arr = env[name]
@@ -210,13 +260,36 @@ class Block:
             return arr[self._index(args, env, box)]
         a = self._value(node[1], env, box)
         b = self._value(node[2], env, box)
+        if _is_r4(a) and _is_r4(b):  # single precision throughout
+            a, b = np.float32(a), np.float32(b)
+        else:  # mixed: the REAL*4 operand is widened exactly
+            a = float(a) if _is_r4(a) else a
+            b = float(b) if _is_r4(b) else b
         if kind == "+":
-            return a + b
-        if kind == "-":
-            return a - b
-        if kind == "*":
-            return a * b
-        return a / b
+            r = a + b
+        elif kind == "-":
+            r = a - b
+        elif kind == "*":
+            r = a * b
+        else:
+            r = a / b
+        return np.float32(r) if (_is_r4(a) and _is_r4(b)) else r
+
+    _CMP = {"EQ": np.equal, "NE": np.not_equal, "GT": np.greater, "LT": np.less, "GE": np.greater_equal,
+            "LE": np.less_equal}
+
+    def _cond(self, cond, env, top, bottom):
+        c = cond.replace(" ", "")
+        if c == "MYPEZ.EQ.0":
+            return top
+        if c == "MYPEZ.EQ.NPEZ-1":
+            return bottom
+        m = re.fullmatch(r"(.+?)\.(EQ|NE|GT|LT|GE|LE)\.(.+)", c)
+        if not m:
+            raise ValueError(f"unsupported condition {cond}")
+        a = self._value(parse(m.group(1)), env, {})
+        b = self._value(parse(m.group(3)), env, {})
+        return bool(self._CMP[m.group(2)](float(a), float(b)))
 
     @staticmethod
     def _refs(node, name):
@@ -234,8 +307,9 @@ class Block:
     def _assign(self, stmt, env, box):
         lhs, rhs = stmt.split("=", 1)
         lt, rt = parse(lhs), parse(rhs)
-        if lt[0] == "id":  # scalar
-            env[lt[1]] = self._value(rt, env, box)
+        if lt[0] == "id":  # scalar (IMPLICIT REAL*8: a REAL*4 value is widened on assignment)
+            v = self._value(rt, env, box)
+            env[lt[1]] = float(v) if _is_r4(v) else v
             return
         name, args = lt[1], lt[2]
         for other in self._refs(rt, name):
@@ -252,6 +326,7 @@ class Block:
         loops: List[Tuple[str, str, int, int]] = []
         body: List[str] = []
         cond_stack: List[bool] = []
+        taken: List[bool] = []  # an earlier branch of the IF at this depth was taken
         for label, st in stmts:
             m = re.fullmatch(r"DO\s*(\d+)\s*([IJK])\s*=\s*(.+?)\s*,\s*(.+)", st)
             if m:
@@ -261,19 +336,24 @@ class Block:
             m = re.fullmatch(r"(ELSE\s*)?IF\s*\((.*)\)\s*THEN", st)
             if m:
                 cond = m.group(2).replace(" ", "")
-                if cond == "MYPEZ.EQ.0":
-                    active = top
-                elif cond == "MYPEZ.EQ.NPEZ-1":
-                    active = bottom
-                else:
-                    raise ValueError(f"unsupported condition {cond}")
+                active = self._cond(cond, env, top, bottom)
                 if m.group(1):
-                    cond_stack[-1] = active  # separate ranks: the two faces are independent
+                    if cond.startswith("MYPEZ"):
+                        cond_stack[-1] = active  # separate ranks: the two faces are independent
+                    else:
+                        taken[-1] = taken[-1] or cond_stack[-1]
+                        cond_stack[-1] = active and not taken[-1]
                 else:
                     cond_stack.append(active)
+                    taken.append(False)
+                continue
+            if st == "ELSE":
+                taken[-1] = taken[-1] or cond_stack[-1]
+                cond_stack[-1] = not taken[-1]
                 continue
             if re.fullmatch(r"END\s*IF", st):
                 cond_stack.pop()
+                taken.pop()
                 continue
             if st == "CONTINUE":
                 if not loops or loops[-1][0] != label:

@@ -64,6 +64,7 @@ class Oracle:
             lib.ora_init.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.ora_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.ora_fluxes.argtypes = [ctypes.c_void_p]
+            lib.ora_heat_loss.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.ora_communicate.argtypes = [ctypes.c_void_p]
             lib.ora_field.restype = ctypes.POINTER(ctypes.c_double)
             lib.ora_field.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -110,6 +111,13 @@ class Oracle:
 
     def communicate(self):
         self.lib().ora_communicate(self.h)
+
+    def heat_loss(self) -> np.ndarray:
+        """The itcon-2 embedded heat-loss term of the current state (FT starting from zeros),
+        shape (NZ, NY, NX)."""
+        out = np.zeros((self.NZ, self.NY, self.NX))
+        self._check(self.lib().ora_heat_loss(self.h, out.ctypes.data))
+        return out
 
     def field(self, name: str) -> np.ndarray:
         """A live view of a 3D field, shape (NZ, NY, NX)."""

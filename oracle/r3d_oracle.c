@@ -566,6 +566,45 @@ int ora_init(ora_sim* s, int seed) {
 #define LOOP_INT for (int k = k1; k <= k2; ++k) for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i)
 #define OMP _Pragma("omp parallel for schedule(static)")
 
+/* Localized embedded heat loss (itcon 2), 3dmhdsub.f:1799-1821: FT -= TP*OCV[*0.5*(1 +
+   TANH(LOG(3)/QFH*(TIMT-TC)))]*RO*EXP(CLN*(EXX-XP)**2)/HH*EXP(CLN*(WYY-YP)**2)/HH*EXP(..ZEE..)/HH
+   over the interior, with RI holding 1/rho (the Fortran's RO at that point).  CLN =
+   -4.0E00*LOG(2.0E00)/HH/HH and LOG(3.0E00) are single-precision literals; x**2 is x*x; TIMT is
+   the time at the start of the step (STEP advances it after the stages). */
+static void heat_loss(ora_sim* s, const double* RI, double* FT) {
+    const ora_params* p = &s->p;
+    const int NX = s->NX, NY = s->NY, NZ = s->NZ;
+    const int i1 = 1, i2 = NX - 2, j1 = 1, j2 = NY - 2, k1 = 1, k2 = NZ - 2;
+    const double *exx = s->line[ORA_EXX], *wyy = s->line[ORA_WYY], *zee = s->line[ORA_ZEE];
+    const double cln = F4(-4.0f * logf(2.0f)) / p->hh / p->hh, hh = p->hh, timt = s->timi + s->timc;
+    OMP for (int k = k1; k <= k2; ++k) for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) {
+        long n = IDX(i, j, k);
+        if (p->tc != 0.0)
+            FT[n] = FT[n] - p->tp * s->ocv * 0.5 * (1.0 + tanh(F4(logf(3.0f)) / p->qfh * (timt - p->tc))) * RI[n] *
+                                exp(cln * ((exx[i] - p->xp) * (exx[i] - p->xp))) / hh *
+                                exp(cln * ((wyy[j] - p->yp) * (wyy[j] - p->yp))) / hh *
+                                exp(cln * ((zee[k] - p->zp) * (zee[k] - p->zp))) / hh;
+        else
+            FT[n] = FT[n] - p->tp * s->ocv * RI[n] * exp(cln * ((exx[i] - p->xp) * (exx[i] - p->xp))) / hh *
+                                exp(cln * ((wyy[j] - p->yp) * (wyy[j] - p->yp))) / hh *
+                                exp(cln * ((zee[k] - p->zp) * (zee[k] - p->zp))) / hh;
+    }
+    (void)NZ;
+}
+
+/* The heat-loss term alone (added to ft, normally zeros) for the current state: the pin of
+   heat_loss against the Fortran block executed statement by statement. */
+int ora_heat_loss(ora_sim* s, double* ft) {
+    const long n = (long)s->NX * s->NY * s->NZ;
+    double* ri = (double*)malloc(sizeof(double) * (size_t)n);
+    if (!ri) { set_err("out of memory"); return -1; }
+    const double* ro = s->f[ORA_RO];
+    for (long q = 0; q < n; ++q) ri[q] = 1.0 / ro[q];
+    heat_loss(s, ri, ft);
+    free(ri);
+    return 0;
+}
+
 static void fluxes(ora_sim* s) {
     const ora_params* p = &s->p;
     const int NX = s->NX, NY = s->NY, NZ = s->NZ;
@@ -650,6 +689,10 @@ static void fluxes(ora_sim* s) {
                 FT[n] += ((A(TT, 0, 0, 1) - A(TT, 0, 0, -1)) * tmpz1 +
                           (A(TT, 0, 0, 1) - 2.0 * TT[n] + A(TT, 0, 0, -1)) * tmpz2) * RO[n] * tmp * rkapa[k];
                 FT[n] += (A(TT, 0, 0, 1) - A(TT, 0, 0, -1)) * hz * dzzdz[k] * RO[n] * tmp * dkapa[k]; } } } }
+
+    /* localized embedded heat loss (itcon 2), after the diffusion and before the viscous terms
+       as in 3dmhdsub.f; RO holds 1/rho at this point (3dmhdsub.f:1405) */
+    if (p->itcon == 2) heat_loss(s, RO, FT);
 
     /* viscous momentum: src/fluxes.cpp:281-320 */
     OMP for (int k = k1; k <= k2; ++k) {
@@ -912,7 +955,7 @@ static int bcon(ora_sim* s) {
 /* src/step.cpp:114-257 (+ B terms of 3dmhdsub.f STEP when lmag). */
 int ora_step(ora_sim* s, int nstages) {
     const ora_params* p = &s->p;
-    if (p->lshr || p->lrem || p->rlax > 0.0 || p->id != 0 || p->itcon == 2 || p->itcon == 3 ||
+    if (p->lshr || p->lrem || p->rlax > 0.0 || p->id != 0 || p->itcon == 3 ||
         p->ixcon != 0 || p->iycon != 0) { set_err("unsupported FLUXES feature"); return -1; }
     const int NX = s->NX, NY = s->NY, NZ = s->NZ;
     const int i1 = 1, i2 = NX - 2, j1 = 1, j2 = NY - 2, k1 = 1, k2 = NZ - 2;

@@ -56,6 +56,10 @@ void ora_mkgrid(ora_sim* s, double scode, int icoord, double* out3);
 /* Copy of the parsed parameters as doubles in a fixed order (see r3d_oracle.c). */
 int ora_param(const ora_sim* s, const char* name, double* out);
 
+/* The itcon-2 embedded heat-loss term of the current state added to ft (test of the
+   restatement against the Fortran block). */
+int ora_heat_loss(ora_sim* s, double* ft);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,6 +37,10 @@ struct Physics {
     double gam[3], zeta[3];
     int lrot, lmag;
     int kappa_const;  // rkapa == 1 and dkapa == 0 on every plane (exact shortcut)
+    // embedded heat loss (itcon 2, 3dmhdsub.f:1799-1821): FT -= heat_pre * (1/rho) * heat_x/HH
+    // * heat_y/HH * heat_z/HH, heat_pre = TP*OCV (tc == 0) or TP*OCV*0.5*(1+tanh(..)) per step
+    int heat_on, hh_one;  // hh_one: HH == 1, where x/HH == x (the divisions are skipped)
+    double heat_pre, hh;
     float gamma_f, ogamma_f, obeta_f;  // float copies for the estimates of the dt filter
 };
 
@@ -47,6 +51,8 @@ struct Lines {
     const double *dzzdz, *d2zzdz2, *tmpz, *tmpz1, *tmpz2;     // [npz+2]
     const double *ddz, *rkapa, *dkapa;                        // [npz+2]
     const double *plume_x, *plume_y;                          // [npx+2], [npy+2]
+    // embedded heat loss (itcon 2): exp(CLN*(x - xp)^2) etc. per line, CLN = f4(-4 ln 2)/HH/HH
+    const double *heat_x, *heat_y, *heat_z;                   // [npx+2], [npy+2], [npz+2]
 };
 
 // Error codes stored in Scalars::err by kernels that abandon a bounded wait.

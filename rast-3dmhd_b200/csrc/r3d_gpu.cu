@@ -370,6 +370,16 @@ double plume_tpr(const r3d_gpu* g) {
     return (g->p.tc != 0.0) ? g->p.tp + (1.0 - g->p.tp) * std::exp(-timt / g->p.tc) : g->p.tp;
 }
 
+// The time factor of the embedded heat loss (itcon 2), 3dmhdsub.f:1801-1818: TP*OCV, ramped by
+// 0.5*(1 + tanh(log(3)/QFH*(TIMT - TC))) when TC != 0; LOG(3.0E00) is a single-precision literal.
+double heat_prefix(const r3d_gpu* g) {
+    const r3d_params& p = g->p;
+    const double tpocv = p.tp * g->ph.ocv;
+    if (p.tc == 0.0) return tpocv;
+    const double timt = g->host_timc + g->host_timi;
+    return tpocv * 0.5 * (1.0 + std::tanh((double)logf(3.0f) / p.qfh * (timt - p.tc)));
+}
+
 void launch_dt_full_any(r3d_gpu* g, int only_refold) {
     if (g->fp32)
         cuda_ok(r3dk::launch_dt_full_fp32(g->geo, g->ph, g->lines, g->bg, fieldset32(g), g->dsc, g->stream,
@@ -384,6 +394,7 @@ void launch_dt_full_any(r3d_gpu* g, int only_refold) {
 void enqueue_step_begin(r3d_gpu* g) {
     Range r("r3d.step_begin");
     g->bnd.tpr = plume_tpr(g);
+    if (g->ph.heat_on) g->ph.heat_pre = heat_prefix(g);
     if (g->halo) halo_reduce_limits(g);
     cuda_ok(r3dk::launch_step_begin(g->ph, g->dsc, g->stream), "step_begin");
 }
@@ -418,6 +429,7 @@ void enqueue_step_end(r3d_gpu* g, int nstages) {
 void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_launches) {
     Range step_range("r3d.step");
     g->bnd.tpr = plume_tpr(g);
+    if (g->ph.heat_on) g->ph.heat_pre = heat_prefix(g);
     tm.begin();
     if (g->halo) halo_reduce_limits(g);
     cuda_ok(r3dk::launch_step_begin(g->ph, g->dsc, g->stream), "step_begin");
@@ -609,10 +621,30 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
         const double a = st->wyy[j] - p.yp;
         py[j] = (p.itcon == 0) ? std::exp(cln * a * a) : std::exp(cln * (a * a));
     }
+    // embedded heat loss profiles (itcon 2, 3dmhdsub.f:1800,1806-1809): the Fortran's
+    // CLN=-4.0E00*LOG(2.0E00)/HH/HH (single-precision literal, then two divisions) and
+    // EXP(CLN*(EXX(I)-XP)**2) with x**2 = x*x; host libm
+    std::vector<double> hx_(NX, 0.0), hy_(NY, 0.0), hz_(NZ, 0.0);
+    if (p.itcon == 2) {
+        const double clh = (double)(-4.0f * logf(2.0f)) / p.hh / p.hh;
+        for (int64_t i = 0; i < NX; ++i) {
+            const double a = st->exx[i] - p.xp;
+            hx_[i] = std::exp(clh * (a * a));
+        }
+        for (int64_t j = 0; j < NY; ++j) {
+            const double a = st->wyy[j] - p.yp;
+            hy_[j] = std::exp(clh * (a * a));
+        }
+        for (int64_t k = 0; k < NZ; ++k) {
+            const double a = st->zee[k] - p.zp;
+            hz_[k] = std::exp(clh * (a * a));
+        }
+    }
     std::vector<const std::vector<double>*> tabs = {&dxxdx, &d2xxdx2, &ddx,  &dyydy, &tmpy,
                                                     &tmpy1, &tmpy2,   &ddy,  &dzzdz, &d2zzdz2,
                                                     &tmpz,  &tmpz1,   &tmpz2, &ddz,  &rkapa,
-                                                    &dkapa, &px,      &py,   &d2yydy2};
+                                                    &dkapa, &px,      &py,   &d2yydy2, &hx_,
+                                                    &hy_,   &hz_};
     size_t total = 0;
     for (auto* t : tabs) total += (t->size() + 15) / 16 * 16;
     if (!g->line_buf) {
@@ -635,6 +667,11 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
     L.dzzdz = dev[8]; L.d2zzdz2 = dev[9]; L.tmpz = dev[10]; L.tmpz1 = dev[11]; L.tmpz2 = dev[12];
     L.ddz = dev[13]; L.rkapa = dev[14]; L.dkapa = dev[15]; L.plume_x = dev[16]; L.plume_y = dev[17];
     L.d2yydy2 = dev[18];
+    L.heat_x = dev[19]; L.heat_y = dev[20]; L.heat_z = dev[21];
+    g->ph.heat_on = p.itcon == 2 ? 1 : 0;
+    g->ph.hh = p.hh;
+    g->ph.hh_one = p.hh == 1.0 ? 1 : 0;
+    g->ph.heat_pre = heat_prefix(g);
     bool kc = true;
     for (int64_t k = 1; k <= NZ - 2; ++k) kc = kc && rkapa[k] == 1.0 && dkapa[k] == 0.0;
     g->ph.kappa_const = kc ? 1 : 0;
@@ -807,9 +844,12 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             ph.kappa_const = 1;
             ph.gamma_f = (float)ph.gamma; ph.ogamma_f = (float)ph.ogamma; ph.obeta_f = (float)ph.obeta;
             r3dk::Boundary& b = g->bnd;
+            // 3dmhdsub.f:2807-2887: a plume for itcon 0/1 with tp != 0, else constant T for itcon
+            // 0 and 2 (the latter with the embedded heat loss in FLUXES), half-domain T for 4,
+            // constant flux for 1
             if (p->tp != 0.0 && (p->itcon == 0 || p->itcon == 1)) b.top_mode = p->itcon == 0 ? 2 : 3;
             else if (p->itcon == 4) b.top_mode = 4;
-            else b.top_mode = p->itcon == 0 ? 0 : 1;
+            else b.top_mode = (p->itcon == 0 || p->itcon == 2) ? 0 : 1;
             b.bottom_mode = p->izcon;
             b.hh = p->hh; b.theta = p->theta; b.tp = p->tp; b.tpr = p->tp;
             b.half_nx = (int)(d.nx / 2);

@@ -350,6 +350,17 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
                     ft += (Tzp - Tzm) * hz * dzk * ri * td * dk;
                 }
 
+                // ---- embedded heat loss (itcon 2), 3dmhdsub.f:1799-1821: RO holds 1/rho there ----
+                if (ph.heat_on) {
+                    double q = ph.heat_pre * ri * L.heat_x[ia];
+                    if (!ph.hh_one) q = q / ph.hh;
+                    q = q * L.heat_y[ja];
+                    if (!ph.hh_one) q = q / ph.hh;
+                    q = q * L.heat_z[k];
+                    if (!ph.hh_one) q = q / ph.hh;
+                    ft = ft - q;
+                }
+
                 // ---- viscous momentum, src/fluxes.cpp:281-320 ----
                 const double ore = ph.ore, c43 = ph.c43;
                 fu += ore * (c43 * ((Uxp - Uxm) * hx * d2x + d2sum(Uxp, U0, Uxm) * h2x * dx1 * dx1) +

@@ -102,16 +102,22 @@ void check_params(const r3d_params& p) {
     if (p.ix != 2 || p.iy != 2 || p.ilap != 2)
         bad("stencil widths --ix/--iy/--ilap must be 2 (the stencil is radius 1)");
     if (p.npx < 3 || p.npy < 3 || p.npz < 5) bad("grid too small: need npx, npy >= 3 and npz >= 5");
-    if (p.ixcon != 0 || p.iycon != 0) bad("non-periodic horizontal boundaries are not supported");
+    if (p.ixcon != 0 || p.iycon != 0)
+        bad("non-periodic horizontal boundaries are not supported (the Fortran FLUXES stops on them too, "
+            "3dmhdsub.f:1267-1280)");
     if (p.lshr) bad("LSHR is not supported (the reference aborts too)");
     if (p.lrem) bad("LREM is not supported (the reference aborts too)");
     if (p.rlax > 0.0) bad("flux relaxation (RLAX) is not supported (the reference aborts too)");
     if (p.id != 0) bad("density diffusion ID is not supported (the reference aborts too)");
-    if (!(p.itcon == 0 || p.itcon == 1 || p.itcon == 4))
-        bad("ITCON must be 0, 1 or 4 (2/3 abort in the reference; others leave the top plane "
-            "undefined)");
+    if (!(p.itcon == 0 || p.itcon == 1 || p.itcon == 2 || p.itcon == 4))
+        bad("ITCON must be 0, 1, 2 or 4 (3 leaves the top temperature to the fluxes, which the fused "
+            "stage kernels do not form on the boundary planes; others leave the top plane undefined)");
+    if (p.itcon == 2 && p.precision != R3D_PREC_FP64)
+        bad("ITCON 2 (embedded heat loss) is available in the fp64 form only");
     if (p.izcon != 0 && p.izcon != 1) bad("IZCON must be 0 or 1");
-    if (p.nstart != 0) bad("restart (nstart != 0) is not supported (the reference aborts too)");
+    if (p.nstart != 0)
+        bad("restart (nstart != 0) is a driver feature: the r3d_b200 command line reads its own gstate "
+            "dumps; the library starts from the state it is given");
     if (p.lmag && p.ntube != 0) bad("TUBE models are not supported (the reference aborts too)");
     if (p.ampb != 0.0 && !p.lmag) bad("AMPB magnetic layer requires LMAG");
     if (p.lmag && (p.rm == 0.0 || p.beta == 0.0)) bad("LMAG needs nonzero --rm and --beta");

@@ -140,6 +140,51 @@ void write_gstate(const r3d_params& p, const HostState& s, const r3d_scalars& sc
     std::fclose(fp);
 }
 
+// Restart (3dmhd.f:289-365, the Fortran driver's NSTART branch; the reference C++ aborts on it,
+// src/main.cpp:150-152): dump number nstart of the NSTEP0-cadence dumps, i.e. the one written at
+// NIT = nstart * nstep0, is read back from this driver's gstate file.  The fields - whole arrays,
+// ghost planes included - replace the initial condition; NIT continues; as in the Fortran, the
+// new run's time origin is TIMI = TIMI + TIMC of the dump with TIMC = 0, and TB is the dumped
+// bottom plane's temperature.
+void read_restart(const r3d_params& p, int nstart, HostState& s, r3d_scalars& sc) {
+    char fname[256];
+    std::snprintf(fname, sizeof fname, "gstate.step.%03d.%04d", 0, nstart * p.nstep0);
+    FILE* fp = std::fopen(fname, "rb");
+    if (!fp) fatal(std::string("rast-3dmhd: restart dump '") + fname + "' not found");
+    auto rd = [&](void* v, size_t n) {
+        if (std::fread(v, 1, n, fp) != n) fatal(std::string("rast-3dmhd: restart dump '") + fname + "' is truncated");
+    };
+    int32_t head[3], hdr[13];
+    double scal[27];
+    rd(head, sizeof head);
+    if (head[0] != 1129928788 || head[1] != 27 || head[2] != 14)
+        fatal(std::string("rast-3dmhd: '") + fname + "' is not a gstate dump");
+    rd(hdr, sizeof hdr);
+    rd(scal, sizeof scal);
+    if (hdr[0] != s.nx || hdr[1] != s.ny || hdr[2] != s.nz || hdr[7] != p.lmag)
+        fatal("rast-3dmhd: restart: grid size mismatch, no interpolation");
+    // the reference's field order: ru rv rw ro tt uu vv ww fu fv fw fr ft zru .. ztt ww1 ww2 ww3 bx by bz ..
+    const int field_of[27] = {0, 1, 2, 3, 4, -1, -1, -1, -1, -1, -1, -1, -1, -1,
+                              -1, -1, -1, -1, -1, -1, -1, 5, 6, 7, -1, -1, -1};
+    const int64_t cnt = s.nx * s.ny * s.nz;
+    std::vector<double> skip((size_t)cnt);
+    for (int q = 0; q < 27; ++q) {
+        int64_t c = 0;
+        rd(&c, 8);
+        if (c != cnt) fatal("rast-3dmhd: restart: bad array length in the dump");
+        const int f = field_of[q];
+        rd(f >= 0 ? s.f[f].data() : skip.data(), (size_t)cnt * 8);
+    }
+    std::fclose(fp);
+    sc.nit = hdr[6];
+    sc.dt = scal[0];
+    sc.timi = scal[3] + scal[1];  // TIMI = PAR1(64) + PAR1(65), 3dmhd.f:330
+    sc.timc = 0.0;
+    sc.timt = sc.timi;
+    sc.umach = scal[4];
+    sc.tb = s.f[4][(size_t)(((s.nz - 2) * s.ny + 1) * s.nx + 1)];  // TB = TT(2,2,NZ-ILAP/2), 3dmhd.f:358
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -166,15 +211,19 @@ int main(int argc, char** argv) {
         fatal("rast-3dmhd: this binary runs the GPU time loop only (--backend gpu); the CPU backend is the "
               "reference build");
     p.backend = 1;
+    const int nstart = p.nstart;  // a driver feature: the library sees a new start
+    if (nstart < 0) fatal("rast-3dmhd: --nstart must be >= 0");
+    p.nstart = 0;
     check(r3d_params_check(&p), "parameter check");
 
     HostState s(p);
     r3d_scalars sc{};
     check(r3d_setup_host(&p, &s.view, &sc), "initial condition");
+    if (nstart > 0) read_restart(p, nstart, s, sc);
     const double dt0 = initial_dt(p, s);
     std::fprintf(stderr, "rast-3dmhd: NP=%d NPEY=%d NPEZ=%d  local %lldx%lldx%lld  NIT0=%d DT=%g NTOTAL=%d\n", 1, 1, 1,
                  (long long)s.nx, (long long)s.ny, (long long)s.nz, p.ntotal, dt0, p.ntotal);
-    if (dump_mode != 0) write_gstate(p, s, sc, "start", 0);
+    if (dump_mode != 0 && nstart == 0) write_gstate(p, s, sc, "start", 0);
 
     struct timespec wstart;
     clock_gettime(CLOCK_MONOTONIC, &wstart);
@@ -212,7 +261,7 @@ int main(int argc, char** argv) {
             }
             const double wall = wall_since();
             std::fprintf(stderr, "NIT %d  DT %g  TIMC %g  UMACH %g  WALL %.1fs (%.2fs/step)\n", sc.nit, sc.dt, sc.timc,
-                         sc.umach, wall, wall / sc.nit);
+                         sc.umach, wall, wall / nk);
         }
     }
     check(r3d_gpu_download(g, &s.view, nullptr), "r3d_gpu_download");

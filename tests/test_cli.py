@@ -98,3 +98,44 @@ def test_gstate_reader_rejects_damaged_files(tmp_path):
         (tmp_path / "bad").write_bytes(bad)
         with pytest.raises(ValueError):
             gstate.read(str(tmp_path / "bad"))
+
+
+def test_cli_restart_refuses_missing_or_mismatched_dumps(tmp_path):
+    """--nstart k reads the dump written at NIT = k * nstep0 (the Fortran driver's dump index,
+    3dmhd.f:289-365); a missing file or another grid is refused before any GPU work."""
+    r = run(["--npx", "8", "--npy", "8", "--npz", "8", "--nstart", "2", "--nstep0", "5"], tmp_path)
+    assert r.returncode != 0 and "gstate.step.000.0010" in r.stderr and "not found" in r.stderr
+    import struct
+    nx, ny, nz = 5, 5, 5  # a dump of another grid
+    parts = [struct.pack("<iii", gstate.MAGIC, 27, 14), struct.pack("<13i", nx, ny, nz, *([0] * 10)),
+             struct.pack("<27d", *([0.5] * 27))]
+    (tmp_path / "gstate.step.000.0010").write_bytes(b"".join(parts))
+    r = run(["--npx", "8", "--npy", "8", "--npz", "8", "--nstart", "2", "--nstep0", "5"], tmp_path)
+    assert r.returncode != 0 and "grid size mismatch" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_restart_continues_the_run_bit_for_bit(tmp_path):
+    """A run restarted from its NIT-5 dump reaches the continuous run's NIT-10 state bit for bit
+    (the dumps hold whole arrays, ghost planes included); time restarts from TIMI = TIMI + TIMC
+    of the dump with TIMC = 0, as in the Fortran driver."""
+    flags = ["--npx", "20", "--npy", "12", "--npz", "24", "--nstep0", "5"]
+    a, b = tmp_path / "continuous", tmp_path / "restarted"
+    a.mkdir()
+    b.mkdir()
+    r = run(flags + ["--ntotal", "10"], a)
+    assert r.returncode == 0, r.stderr
+    r = run(flags + ["--ntotal", "5"], b)
+    assert r.returncode == 0, r.stderr
+    r = run(flags + ["--ntotal", "5", "--nstart", "1"], b)
+    assert r.returncode == 0, r.stderr
+    assert [ln.split()[1] for ln in r.stderr.splitlines() if ln.startswith("NIT ")] == ["10"]
+    ga = gstate.read(str(a / "gstate.step.000.0010"))
+    gb = gstate.read(str(b / "gstate.step.000.0010"))
+    assert ga.header == gb.header and ga.header["nit"] == 10
+    for n in ("ru", "rv", "rw", "ro", "tt", "zru", "zrv", "zrw", "zro", "ztt"):
+        assert np.array_equal(ga.fields[n], gb.fields[n]), n
+    assert ga.scalars["dt"] == gb.scalars["dt"]
+    g5 = gstate.read(str(b / "gstate.step.000.0005"))
+    assert gb.scalars["timi"] == g5.scalars["timi"] + g5.scalars["timc"]
+    assert abs(gb.scalars["timi"] + gb.scalars["timc"] - ga.scalars["timc"]) <= 1e-14 * ga.scalars["timc"]

@@ -28,6 +28,13 @@ HYDRO_CASES = [
     ("itcon4", ["--npx", "24", "--npy", "16", "--npz", "40", "--itcon", "4"], 3, 4),
     ("no_plume", ["--npx", "24", "--npy", "16", "--npz", "40", "--tp", "0"], 3, 4),
     ("min_size", ["--npx", "3", "--npy", "3", "--npz", "8"], 2, 3),
+    # itcon 2: constant top T and the localized embedded heat loss of the Fortran FLUXES
+    # (3dmhdsub.f:1799-1822; the oracle's term is pinned to that source, test_oracle_itc2_pin.py)
+    ("itcon2_heat_loss", ["--npx", "24", "--npy", "20", "--npz", "36", "--itcon", "2", "--tp", "0.5",
+                          "--xp", "8", "--yp", "12", "--zp", "0.1"], 5, 5),
+    ("itcon2_ramp_hh07", ["--npx", "21", "--npy", "17", "--npz", "30", "--itcon", "2", "--tp", "0.3",
+                          "--tc", "0.002", "--qfh", "0.001", "--hh", "0.7", "--xp", "6", "--yp", "9",
+                          "--zp", "0.3"], 7, 6),
 ]
 
 
