@@ -955,7 +955,7 @@ static int bcon(ora_sim* s) {
 /* src/step.cpp:114-257 (+ B terms of 3dmhdsub.f STEP when lmag). */
 int ora_step(ora_sim* s, int nstages) {
     const ora_params* p = &s->p;
-    if (p->lshr || p->lrem || p->rlax > 0.0 || p->id != 0 || p->itcon == 3 ||
+    if (p->lshr || p->lrem || p->rlax > 0.0 || p->id != 0 ||
         p->ixcon != 0 || p->iycon != 0) { set_err("unsupported FLUXES feature"); return -1; }
     const int NX = s->NX, NY = s->NY, NZ = s->NZ;
     const int i1 = 1, i2 = NX - 2, j1 = 1, j2 = NY - 2, k1 = 1, k2 = NZ - 2;

@@ -250,7 +250,8 @@ dim3 cell_grid(const r3d_gpu* g) {
 Adjoint* workspace(r3d_gpu* g) {
     if (g->adj) return g->adj;
     if (g->fp32) throw Error(R3D_EINVAL, "the adjoint is available for precision fp64 only");
-    if (g->p.itcon == 2) throw Error(R3D_EINVAL, "the adjoint does not include the embedded heat loss (itcon 2)");
+    if (g->p.itcon == 2 || g->p.itcon == 3)
+        throw Error(R3D_EINVAL, "the adjoint covers itcon 0, 1 and 4 (not the embedded heat loss or a free top T)");
     if (g->nloc != g->p.npz || g->halo) throw Error(R3D_EINVAL, "the adjoint needs the whole domain on one handle");
     if (g->p.tp != 0.0 && g->p.tc != 0.0 && (g->p.itcon == 0 || g->p.itcon == 1))
         throw Error(R3D_EINVAL, "the adjoint needs a time-independent top boundary (tc == 0)");

@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(256) bcon_kernel(Geometry g, Physics ph, Lines
                     t = c43 * tt[n + P] - c13 * tt[n + 2 * P] -
                         c23 * b.dz_top * (b.theta - (b.theta - b.tpr) * L.plume_x[i] / b.hh * L.plume_y[j] / b.hh);
                     break;
+                case 5: t = tt[n]; break;  // itcon 3: the stage's value stands
                 default: t = (i <= b.half_nx) ? 1.0 - b.tp : 1.0; break;
             }
             put_periodic(ru, P, g, i, j, u);

@@ -40,6 +40,7 @@ struct Physics {
     // embedded heat loss (itcon 2, 3dmhdsub.f:1799-1821): FT -= heat_pre * (1/rho) * heat_x/HH
     // * heat_y/HH * heat_z/HH, heat_pre = TP*OCV (tc == 0) or TP*OCV*0.5*(1+tanh(..)) per step
     int heat_on, hh_one;  // hh_one: HH == 1, where x/HH == x (the divisions are skipped)
+    int top_free;         // itcon 3: BCON leaves the top temperature; its flux is formed there
     double heat_pre, hh;
     float gamma_f, ogamma_f, obeta_f;  // float copies for the estimates of the dt filter
 };
@@ -60,7 +61,8 @@ enum { kErrNone = 0, kErrTmaTimeout = 1 };
 
 // Boundary set-up for the BCON kernel (src/bcon.cpp:12-141).
 struct Boundary {
-    int top_mode;     // 0 const T=1, 1 const flux, 2 plume T, 3 plume flux, 4 half-domain T
+    int top_mode;     // 0 const T=1, 1 const flux, 2 plume T, 3 plume flux, 4 half-domain T,
+                      // 5 free (itcon 3: T evolves with its own flux, 3dmhdsub.f:2807-2887)
     int bottom_mode;  // 0 const T=tb, 1 const flux
     double tpr, hh, theta, tp, dz_top, dz_bot, tb;
     int half_nx;      // NX/2 for ITCON 4

@@ -849,7 +849,9 @@ r3d_gpu* create_handle(const r3d_params& pin, int z0, int nloc, cudaStream_t sha
             // constant flux for 1
             if (p->tp != 0.0 && (p->itcon == 0 || p->itcon == 1)) b.top_mode = p->itcon == 0 ? 2 : 3;
             else if (p->itcon == 4) b.top_mode = 4;
+            else if (p->itcon == 3) b.top_mode = 5;
             else b.top_mode = (p->itcon == 0 || p->itcon == 2) ? 0 : 1;
+            g->ph.top_free = p->itcon == 3 ? 1 : 0;
             b.bottom_mode = p->izcon;
             b.hh = p->hh; b.theta = p->theta; b.tp = p->tp; b.tpr = p->tp;
             b.half_nx = (int)(d.nx / 2);

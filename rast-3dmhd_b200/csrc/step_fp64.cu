@@ -64,9 +64,15 @@ constexpr int NRAW = 4, NDER = 4;
 // carries CPT independent stencil evaluations (and shares the y-neighbour loads between them).
 // Two rows in the first two stages, one in the third (its filtered dt epilogue branches per
 // cell); an MHD cell already needs most of the register file, so MHD threads take one row.
-template <bool B>
+// The right-hand side's variant of a plane: interior, or a domain edge (one-sided continuity
+// and B stencils; the momentum and energy fluxes, which BCON rewrites, not formed) - or, with
+// FULL, the top edge whose temperature BCON leaves alone (itcon 3): one-sided continuity and
+// every momentum and energy flux formed as on an interior plane, as the reference does on its
+// edge planes (src/fluxes.cpp loops over k1..k2).
+template <bool B, bool FULL = false>
 struct EdgeTag {
     static constexpr bool value = B;
+    static constexpr bool full = FULL;
 };
 
 // xp - 2.0 * x0 + xm in the reference's rounding, rn(rn(xp - rn(2 * x0)) + xm), with one FP64
@@ -112,7 +118,8 @@ void stage_fp64_box(int rows, unsigned* bx, unsigned* by) {
     *by = rows + 2;
 }
 
-template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV>
+// TF (hydro, itcon 3 only): the top plane's flux is formed as on an interior plane (EdgeTag)
+template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV, bool TF = false>
 __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::min_blocks)
     stage_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
                FieldSet fs, Scalars* sc, int kchunk) {
@@ -260,6 +267,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
         // per case, so that the rows' evaluations share basic blocks
         auto rhs = [&](auto edge_tag) {
           constexpr bool EDGE = decltype(edge_tag)::value;
+          constexpr bool FULLTOP = decltype(edge_tag)::full;
 #pragma unroll
           for (int c = 0; c < CPT; ++c) {
 #pragma unroll
@@ -307,7 +315,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
             const double vz = (Vzp - Vzm) * hz * dzk;  // :469; 3dmhdsub.f:2217
             const double wz = (Wzp - Wzm) * hz * dzk;  // :423; 3dmhdsub.f:2223
 
-            if (!EDGE) {
+            if (!EDGE || FULLTOP) {
                 const double tmpz1 = L.tmpz1[k], tmpz2 = L.tmpz2[k];
                 const double T0 = RW_(r0, R_TT, 0, 0);
 
@@ -524,8 +532,16 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
             }
           }
         };
-        if (edge) rhs(EdgeTag<true>{});
-        else rhs(EdgeTag<false>{});
+        if (!edge) {
+            rhs(EdgeTag<false>{});
+        } else {
+            if constexpr (TF && !MHD) {
+                if (k == 1 && g.top_edge) rhs(EdgeTag<true, true>{});
+                else rhs(EdgeTag<true>{});
+            } else {
+                rhs(EdgeTag<true>{});
+            }
+        }
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
           if (actv[c]) {
@@ -596,36 +612,42 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
     if (STAGE == 2) reduce_dt(der, m1, m2, m3, m4, mu, sc);
 }
 
-template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV>
+template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV, bool TF>
 static void launch_one(dim3 grid, const StageMaps& maps, const Geometry& g, const Physics& ph,
                        const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
     static bool configured = false;
     constexpr size_t smem = Shape<MHD, TYV>::smem;
     if (!configured) {
-        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         configured = true;
     }
     const dim3 block(TX, TYV / Cells<MHD, STAGE, TYV>::cpt, 1);
-    stage_fp64<STAGE, KC, MHD, EMIT, TYV><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
+    stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
 }
 
-template <bool MHD, bool EMIT, int TYV>
+template <bool MHD, bool EMIT, int TYV, bool TF = false>
 static void launch_stage(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                          const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
     const dim3 grid((g.npx + TX - 1) / TX, (g.npy + TYV - 1) / TYV, (g.npz + kchunk - 1) / kchunk);
     const bool kc = ph.kappa_const != 0;
-    if (stage == 0) kc ? launch_one<0, true, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st)
-                       : launch_one<0, false, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st);
-    else if (stage == 1) kc ? launch_one<1, true, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st)
-                            : launch_one<1, false, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st);
-    else kc ? launch_one<2, true, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st)
-            : launch_one<2, false, MHD, EMIT, TYV>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+    if (stage == 0) kc ? launch_one<0, true, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+                       : launch_one<0, false, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+    else if (stage == 1) kc ? launch_one<1, true, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+                            : launch_one<1, false, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+    else kc ? launch_one<2, true, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+            : launch_one<2, false, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st);
 }
 
 template <bool EMIT>
 static void launch_any(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                        const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
+    if constexpr (!EMIT) {  // itcon 3 (hydro; the adjoint's EMIT recompute refuses it)
+        if (!ph.lmag && ph.top_free) {
+            launch_stage<false, false, R3D_STAGE_TY, true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+            return;
+        }
+    }
     if (!ph.lmag) launch_stage<false, EMIT, R3D_STAGE_TY>(stage, maps, g, ph, L, fs, sc, kchunk, st);
     else if (g.tile_rows == 6) launch_stage<true, EMIT, 6>(stage, maps, g, ph, L, fs, sc, kchunk, st);
     else launch_stage<true, EMIT, 8>(stage, maps, g, ph, L, fs, sc, kchunk, st);

@@ -109,11 +109,11 @@ void check_params(const r3d_params& p) {
     if (p.lrem) bad("LREM is not supported (the reference aborts too)");
     if (p.rlax > 0.0) bad("flux relaxation (RLAX) is not supported (the reference aborts too)");
     if (p.id != 0) bad("density diffusion ID is not supported (the reference aborts too)");
-    if (!(p.itcon == 0 || p.itcon == 1 || p.itcon == 2 || p.itcon == 4))
-        bad("ITCON must be 0, 1, 2 or 4 (3 leaves the top temperature to the fluxes, which the fused "
-            "stage kernels do not form on the boundary planes; others leave the top plane undefined)");
+    if (!(p.itcon >= 0 && p.itcon <= 4)) bad("ITCON must be 0 .. 4 (others leave the top plane undefined)");
     if (p.itcon == 2 && p.precision != R3D_PREC_FP64)
         bad("ITCON 2 (embedded heat loss) is available in the fp64 form only");
+    if (p.itcon == 3 && (p.precision != R3D_PREC_FP64 || p.lmag))
+        bad("ITCON 3 (free top temperature) is available in the fp64 hydro form only");
     if (p.izcon != 0 && p.izcon != 1) bad("IZCON must be 0 or 1");
     if (p.nstart != 0)
         bad("restart (nstart != 0) is a driver feature: the r3d_b200 command line reads its own gstate "

@@ -35,6 +35,13 @@ HYDRO_CASES = [
     ("itcon2_ramp_hh07", ["--npx", "21", "--npy", "17", "--npz", "30", "--itcon", "2", "--tp", "0.3",
                           "--tc", "0.002", "--qfh", "0.001", "--hh", "0.7", "--xp", "6", "--yp", "9",
                           "--zp", "0.3"], 7, 6),
+    # itcon 3: the top temperature is the stage's own (no BCON rewrite, 3dmhdsub.f:2807-2880), so
+    # the top plane's energy flux is formed in full; both conductivity forms, with rotation
+    ("itcon3_free_top", ["--npx", "24", "--npy", "20", "--npz", "36", "--itcon", "3", "--tp", "0.5",
+                         "--lrot", "1", "--ry", "2", "--ang", "0.3"], 5, 6),
+    ("itcon3_variable_kappa_izcon1", ["--npx", "21", "--npy", "17", "--npz", "30", "--itcon", "3",
+                                      "--izcon", "1", "--ngrid", "2", "--pzp", "0.5", "--sigma", "0.1",
+                                      "--polys", "1.5"], 7, 5),
 ]
 
 

@@ -76,13 +76,14 @@ def test_parser_rejects_unknown_and_missing_values():
 @pytest.mark.parametrize("args,msg", [
     (["--ix", "4"], "stencil"), (["--lrem", "1"], "LREM"), (["--lshr", "1"], "LSHR"),
     (["--rlax", "0.5"], "RLAX"), (["--id", "1"], "ID"), (["--itcon", "2", "--precision", "fp32bulk"], "ITCON 2"),
-    (["--itcon", "3"], "ITCON"), (["--izcon", "2"], "IZCON"), (["--ixcon", "1"], "periodic"),
+    (["--itcon", "3", "--precision", "fp32bulk"], "ITCON 3"), (["--itcon", "3", "--lmag", "1"], "ITCON 3"),
+    (["--itcon", "5"], "ITCON"), (["--izcon", "2"], "IZCON"), (["--ixcon", "1"], "periodic"),
     (["--nstart", "3"], "restart"), (["--ampb", "0.1"], "AMPB"),
     (["--lmag", "1", "--rm", "0", "--beta", "1"], "LMAG"), (["--seed", "0"], "seed"),
     (["--npz", "4"], "too small"),
 ])
 def test_unsupported_configurations_are_errors(args, msg):
-    """Configurations this build refuses, with the reason (ITCON 2 runs in the fp64 form)."""
+    """Configurations this build refuses, with the reason (ITCON 2 and 3 run in the fp64 form)."""
     with pytest.raises(R.R3dError) as e:
         R.check(R.parse(args))
     assert e.value.code == R.R3D_EINVAL and msg in str(e.value)
