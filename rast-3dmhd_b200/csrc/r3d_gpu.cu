@@ -241,7 +241,8 @@ int stage_chunk_depth(const r3d_params& p, bool fp32, int tile_rows, int nloc, i
     if (fp32) r3dk::stage_fp32_box(&tbx, &tby);
     else r3dk::stage_fp64_box(tile_rows, &tbx, &tby);
     const int64_t tiles = (int64_t)((p.npx + 31) / 32) * ((p.npy + (int)tby - 3) / ((int)tby - 2));
-    const int64_t slots = (int64_t)num_sms * (fp32 ? r3dk::stage_fp32_ctas_per_sm() : 2 - (p.lmag && tby == 10 ? 1 : 0));
+    const int64_t slots = (int64_t)num_sms * (fp32 ? r3dk::stage_fp32_ctas_per_sm()
+                                                   : r3dk::stage_fp64_ctas_per_sm(p.lmag, (int)tby - 2));
     if (p.lmag && tby == 8) {
         // 32x6 MHD tiles, two CTAs per SM: 12-plane chunks.  Measured on B200 against the
         // earlier 16/32-plane choice: 126x126x256 0.962 -> 0.922 ms per step, 252x252x256

@@ -61,6 +61,8 @@ size_t stage_fp64_smem();
 // Rows of the FP64 stage kernel's column tiles for a grid (8 hydro; MHD 6, or 8 on grids too
 // small for two CTAs per SM), and the TMA box (x, y) of one field plane for tiles of that height.
 int stage_fp64_rows(int mhd, int npx, int npy, int nloc, int num_sms);
+// resident CTAs per SM of the FP64 stage kernels (hydro: all three stages; MHD: by tile rows)
+int stage_fp64_ctas_per_sm(int mhd, int rows);
 void stage_fp64_box(int rows, unsigned* bx, unsigned* by);
 cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
                               const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,

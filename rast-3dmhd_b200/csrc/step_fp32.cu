@@ -101,7 +101,7 @@ template <int STAGE>
 __global__ void __launch_bounds__(Sh::NT, STAGE == 2 ? Sh::ctas_s2 : Sh::ctas)
     stage_fp32(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L, Background bg,
                FieldSet32 fs, Scalars* sc, int kchunk) {
-    constexpr int SY = Sh::SY, NT = Sh::NT, RAWF = Sh::RAWF, DERF = Sh::DERF;
+    constexpr int NT = Sh::NT, RAWF = Sh::RAWF, DERF = Sh::DERF;
     constexpr int RAW_SLOT = Sh::RAW_SLOT, DER_SLOT = Sh::DER_SLOT;
     extern __shared__ __align__(128) unsigned char smem[];
     float* raw = reinterpret_cast<float*>(smem);

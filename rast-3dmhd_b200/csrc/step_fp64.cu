@@ -15,13 +15,15 @@
 //
 // Pipeline: a CTA owns a 32 x TY column tile (TY = 8 hydro; 6, or 8 on small grids, with MHD)
 // and marches down a chunk of z planes (depth chosen per handle on the host).  Thread 0
-// streams the state fields of each plane, with a one-cell x/y halo, into a 4-slot ring by TMA
-// (one (34, TY+2, 1) box per field, completion on a per-slot mbarrier), two planes ahead of
-// the plane being computed.  Each loaded cell is then turned once into 1/rho, u, v, w and
-// P = rho*T (src/fluxes.cpp:131-166) in a second 4-slot ring, so a single __syncthreads per
-// plane orders everything: the plane k+1 derivation, the TMA refill of the slot of plane k-2,
-// and the compute of plane k, which reads the 19-point stencil (the twelve edge neighbours of
-// u, v, w come from the cross terms :367-374, :449-456, :496-498) from shared memory.
+// streams the state fields of each plane, with a one-cell x/y halo, into a ring by TMA (one
+// (34, TY+2, 1) box per field, completion on a per-slot mbarrier), two planes ahead of the
+// plane being computed.  Each loaded cell is then turned once into u, v, w (and, with MHD,
+// 1/rho and P = rho*T; src/fluxes.cpp:131-166) in a second, 4-slot ring, so a single
+// __syncthreads per plane orders everything: the plane k+1 derivation, the TMA refill of the
+// slot of plane k-2 (hydro: of plane k-1, whose values the threads hold), and the compute of
+// plane k, which reads the 19-point stencil (the twelve edge neighbours of u, v, w come from
+// the cross terms :367-374, :449-456, :496-498) from shared memory.  Hydro threads compute two
+// adjacent rows each, 128-thread CTAs, three per SM; MHD threads one row.
 // Planes k = 1 and k = npz carry only the continuity flux and, with MHD, the Bx/By fluxes:
 // their momenta, T and Bz are rewritten by BCON (src/bcon.cpp:27-140); the one-sided
 // z-derivatives there (src/fluxes.cpp:106-117, 3dmhdsub.f:2245-2259, 2468-2487, 2577-2596)
@@ -31,6 +33,8 @@
 // limits of the next step (src/step.cpp:122-229).
 #include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "r3d_kernels.h"
 #include "stage_common.cuh"
@@ -49,7 +53,7 @@
 #define R3D_CPT_S1 2
 #endif
 #ifndef R3D_CPT_S2
-#define R3D_CPT_S2 1  // the third stage's dt epilogue runs better with one row per thread
+#define R3D_CPT_S2 2
 #endif
 
 namespace r3dk {
@@ -58,7 +62,26 @@ namespace {
 constexpr int TX = 32, SX = TX + 2;
 enum { R_RU, R_RV, R_RW, R_RO, R_TT, R_BX, R_BY, R_BZ };
 enum { D_U, D_V, D_W, D_P, D_RI, D_NF };
-constexpr int NRAW = 4, NDER = 4;
+constexpr int NDER = 4;
+#ifndef R3D_ZAHEAD
+#define R3D_ZAHEAD 1  // planes by which the L2 prefetch of the accumulators runs ahead
+#endif
+// Hydro keeps a lean shared-memory layout, so that three 128-thread CTAs fit on an SM: a 3-slot
+// raw ring (the thread's own values of plane k-1 are carried in registers), and u, v, w only in
+// the derived ring (1/rho of the thread's own cells stays in registers; P = rho*T is formed
+// where it is used, the product the reference stores).  MHD keeps the 4-slot raw ring and the
+// derived u, v, w, P, 1/rho.  Both prefetch the RK accumulators of the next plane into L2 and
+// load a plane's accumulators when its computation starts, which takes fewer registers than
+// holding the next plane's values in registers (hydro: 40; measured on B200 at 1965 MHz:
+// 504x504x512 hydro 15.45 -> 15.06 ms per step, 126x126x256 MHD 0.946 -> 0.901 ms; a prefetch
+// two planes ahead: hydro 15.2-15.3 ms).
+template <bool MHD>
+struct Ring {
+    static constexpr bool lean = !MHD;
+    static constexpr int nraw = lean ? 3 : 4;
+    static constexpr int nder_f = lean ? 3 : D_NF;  // derived fields per slot
+    static constexpr bool z_l2 = true;
+};
 
 // Cells per thread: a hydro thread computes CPT adjacent rows of its tile column, so each warp
 // carries CPT independent stencil evaluations (and shares the y-neighbour loads between them).
@@ -90,12 +113,14 @@ struct Shape {
     static constexpr int rawf = (sn + 15) / 16 * 16;  // doubles per raw field box, 128 B multiple
     static constexpr int nf = MHD ? 8 : 5;                 // raw fields per plane
     static constexpr int raw_slot = nf * rawf;             // doubles
-    static constexpr int der_slot = D_NF * sn;             // doubles
-    static constexpr size_t raw_bytes = (size_t)NRAW * raw_slot * sizeof(double);
+    static constexpr int der_slot = Ring<MHD>::nder_f * sn;  // doubles
+    static constexpr size_t raw_bytes = (size_t)Ring<MHD>::nraw * raw_slot * sizeof(double);
     static constexpr size_t der_bytes = (size_t)NDER * der_slot * sizeof(double);
     static constexpr uint32_t plane_tx = nf * sn * sizeof(double);  // TMA bytes per plane
     static constexpr size_t smem = raw_bytes + der_bytes + 64;
     static constexpr int min_blocks = (smem * 2 <= 227 * 1024 && TX * ty <= 256) ? 2 : 1;
+    // resident CTAs per SM of a 128-thread hydro CTA (two rows per thread)
+    static constexpr int min_blocks_lean = (smem + 1024) * 3 <= 228 * 1024 ? 3 : min_blocks;
     static_assert(raw_bytes % 128 == 0 && (rawf * 8) % 128 == 0, "TMA destinations 128-byte aligned");
 };
 
@@ -103,11 +128,18 @@ template <bool MHD, int STAGE, int TYV>
 struct Cells {
     static constexpr int cpt = MHD ? 1 : (STAGE == 0 ? R3D_CPT_S0 : (STAGE == 1 ? R3D_CPT_S1 : R3D_CPT_S2));
     static constexpr int nt = TX * TYV / cpt;  // threads per CTA
+    static constexpr int min_blocks =
+        (!MHD && nt <= 128) ? Shape<MHD, TYV>::min_blocks_lean : Shape<MHD, TYV>::min_blocks;
     static_assert(TYV % cpt == 0, "tile rows must divide among the threads");
 };
 }  // namespace
 
 size_t stage_fp64_smem() { return Shape<false, R3D_STAGE_TY>::smem; }
+int stage_fp64_ctas_per_sm(int mhd, int rows) {
+    if (!mhd) return std::min({Cells<false, 0, R3D_STAGE_TY>::min_blocks, Cells<false, 1, R3D_STAGE_TY>::min_blocks,
+                               Cells<false, 2, R3D_STAGE_TY>::min_blocks});
+    return rows == 6 ? Shape<true, 6>::min_blocks : Shape<true, 8>::min_blocks;
+}
 int stage_fp64_rows(int mhd, int npx, int npy, int nloc, int num_sms) {
     if (!mhd) return R3D_STAGE_TY;
     const long tiles6 = (long)((npx + TX - 1) / TX) * ((npy + 5) / 6);
@@ -120,7 +152,7 @@ void stage_fp64_box(int rows, unsigned* bx, unsigned* by) {
 
 // TF (hydro, itcon 3 only): the top plane's flux is formed as on an interior plane (EdgeTag)
 template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV, bool TF = false>
-__global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::min_blocks)
+__global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, TYV>::min_blocks)
     stage_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
                FieldSet fs, Scalars* sc, int kchunk) {
     using S = Shape<MHD, TYV>;
@@ -141,7 +173,16 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
     const int ke = min(g.npz, kb + kchunk - 1);
     const int i = i0 + tx, jr = j0 + ty * CPT;  // the thread's column and first row
 
-    // plane p has local index q = p - (kb - 1); ring slot q % 4, mbarrier phase (q / 4) & 1
+    constexpr bool LEAN = Ring<MHD>::lean;
+    constexpr bool ZL2 = Ring<MHD>::z_l2;
+    constexpr int NRAW = Ring<MHD>::nraw;
+    // the thread's own cells in the halo tile (row c of the thread: halo row ty*CPT + c + 1)
+    const int own0 = (ty * CPT + 1) * SX + tx + 1;
+    // lean layout: 1/rho of the own cells of the plane derived last (rin) and of the plane
+    // being computed (riq)
+    double rin[CPT], riq[CPT];
+
+    // plane p has local index q = p - (kb - 1); ring slot q % NRAW, mbarrier phase (q / NRAW) & 1
     int last_issued = kb - 2, last_waited = kb - 2;  // bookkeeping of thread 0 for the drain
     unsigned int tx_extra = 0;                          // read by thread 0 (test hook, normally 0)
     auto issue = [&](int p) {
@@ -159,14 +200,37 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
         last_waited = p;
         const double* r = raw + (q % NRAW) * S::raw_slot;
         double* d = der + (q % NDER) * S::der_slot;
-        for (int c = tid; c < SN; c += NTH) {
-            const double ro = r[R_RO * RAWF + c];
-            const double ri = __drcp_rn(ro);  // == 1.0/ro, src/fluxes.cpp:137
-            d[D_U * SN + c] = r[R_RU * RAWF + c] * ri;          // src/fluxes.cpp:158
-            d[D_V * SN + c] = r[R_RV * RAWF + c] * ri;          // src/fluxes.cpp:162
-            d[D_W * SN + c] = r[R_RW * RAWF + c] * ri;          // src/fluxes.cpp:166
-            d[D_P * SN + c] = ro * r[R_TT * RAWF + c];          // src/fluxes.cpp:136
-            d[D_RI * SN + c] = ri;
+        if constexpr (LEAN) {
+            // every thread its own cells (keeping their 1/rho), then the halo ring of the tile:
+            // the top and bottom halo rows, then the left and right halo columns
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+                const int n = own0 + c * SX;
+                const double ri = __drcp_rn(r[R_RO * RAWF + n]);  // == 1.0/ro, src/fluxes.cpp:137
+                d[D_U * SN + n] = r[R_RU * RAWF + n] * ri;        // src/fluxes.cpp:158
+                d[D_V * SN + n] = r[R_RV * RAWF + n] * ri;        // src/fluxes.cpp:162
+                d[D_W * SN + n] = r[R_RW * RAWF + n] * ri;        // src/fluxes.cpp:166
+                rin[c] = ri;
+            }
+            constexpr int NHALO = 2 * SX + 2 * TY;
+            for (int h = tid; h < NHALO; h += NTH) {
+                const int e = h - 2 * SX;
+                const int n = (h < SX) ? h : ((h < 2 * SX) ? (TY + 1) * SX + (h - SX) : (1 + (e >> 1)) * SX + ((e & 1) ? SX - 1 : 0));
+                const double ri = __drcp_rn(r[R_RO * RAWF + n]);
+                d[D_U * SN + n] = r[R_RU * RAWF + n] * ri;
+                d[D_V * SN + n] = r[R_RV * RAWF + n] * ri;
+                d[D_W * SN + n] = r[R_RW * RAWF + n] * ri;
+            }
+        } else {
+            for (int c = tid; c < SN; c += NTH) {
+                const double ro = r[R_RO * RAWF + c];
+                const double ri = __drcp_rn(ro);  // == 1.0/ro, src/fluxes.cpp:137
+                d[D_U * SN + c] = r[R_RU * RAWF + c] * ri;          // src/fluxes.cpp:158
+                d[D_V * SN + c] = r[R_RV * RAWF + c] * ri;          // src/fluxes.cpp:162
+                d[D_W * SN + c] = r[R_RW * RAWF + c] * ri;          // src/fluxes.cpp:166
+                d[D_P * SN + c] = ro * r[R_TT * RAWF + c];          // src/fluxes.cpp:136
+                d[D_RI * SN + c] = ri;
+            }
         }
         return true;
     };
@@ -191,6 +255,17 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
         issue(kb + 1);
     }
     bool ok = derive(kb - 1);
+    // lean layout: the own cells' values of the plane above the chunk (rho, T and the momenta,
+    // the k-1 neighbours of its first plane), carried in registers from plane to plane
+    double cm[CPT][5];
+    if constexpr (LEAN) {
+        if (ok) {
+#pragma unroll
+            for (int c = 0; c < CPT; ++c)
+#pragma unroll
+                for (int f = 0; f < 5; ++f) cm[c][f] = raw[f * RAWF + own0 + c * SX];  // slot 0: plane kb-1
+        }
+    }
     ok = derive(kb) && ok;
     if (!ok) s_abort = 1;
 
@@ -223,7 +298,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f) zn[c][f] = 0.0;
-        if (STAGE > 0 && actv[c]) {
+        if (STAGE > 0 && actv[c] && !ZL2) {
 #pragma unroll
             for (int f = 0; f < NF; ++f) zn[c][f] = fs.z[f][kb * PL + colv[c]];
         }
@@ -234,14 +309,27 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
         // the next plane's accumulators: issued before the derive phase and the barrier, so
         // their latency hides behind a whole plane of work
         double zq[CPT][NF];
+        if constexpr (!ZL2) {
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) {
+            for (int c = 0; c < CPT; ++c) {
 #pragma unroll
-            for (int f = 0; f < NF; ++f) zq[c][f] = zn[c][f];
-            if (STAGE > 0 && actv[c] && k < ke) {
+                for (int f = 0; f < NF; ++f) zq[c][f] = zn[c][f];
+                if (STAGE > 0 && actv[c] && k < ke) {
 #pragma unroll
-                for (int f = 0; f < NF; ++f) zn[c][f] = fs.z[f][(k + 1) * PL + colv[c]];
+                    for (int f = 0; f < NF; ++f) zn[c][f] = fs.z[f][(k + 1) * PL + colv[c]];
+                }
             }
+        } else if (STAGE > 0 && k + R3D_ZAHEAD <= ke) {
+#pragma unroll
+            for (int c = 0; c < CPT; ++c)
+                if (actv[c]) {
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) prefetch_l2(fs.z[f] + (k + R3D_ZAHEAD) * PL + colv[c]);
+                }
+        }
+        if constexpr (LEAN) {
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) riq[c] = rin[c];
         }
         if (!derive(k + 1)) s_abort = 1;
         __syncthreads();
@@ -249,6 +337,17 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
         if (tid == 0 && k + 2 <= ke + 1) {
             fence_proxy_async();
             issue(k + 2);
+        }
+        if constexpr (ZL2) {  // this plane's accumulators, from L2, consumed by the stage update
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+#pragma unroll
+                for (int f = 0; f < NF; ++f) zq[c][f] = 0.0;
+                if (STAGE > 0 && actv[c]) {
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) zq[c][f] = fs.z[f][k * PL + colv[c]];
+                }
+            }
         }
         const double* rm = raw + ((q + NRAW - 1) % NRAW) * S::raw_slot;
         const double* r0 = raw + (q % NRAW) * S::raw_slot;
@@ -258,6 +357,11 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
         const double* dp = der + ((q + 1) % NDER) * S::der_slot;
 #define RW_(P, F, DX, DY) P[(F)*RAWF + s0 + (DY)*SX + (DX)]
 #define DV_(P, F, DX, DY) P[(F)*SN + s0 + (DY)*SX + (DX)]
+// own-cell raw value of plane k-1; P = rho*T on planes k (with x/y offsets), k+1 and k-1
+#define RM_(F) (LEAN ? cm[c][F] : RW_(rm, F, 0, 0))
+#define P0_(DX, DY) (LEAN ? RW_(r0, R_RO, DX, DY) * RW_(r0, R_TT, DX, DY) : DV_(d0, D_P, DX, DY))
+#define PP_ (LEAN ? RW_(rp, R_RO, 0, 0) * RW_(rp, R_TT, 0, 0) : DV_(dp, D_P, 0, 0))
+#define PM_ (LEAN ? cm[c][R_RO] * cm[c][R_TT] : DV_(dm, D_P, 0, 0))
         const double tmpz = L.tmpz[k];
         const bool edge = (k == 1 && g.top_edge) || (k == g.npz && g.bot_edge);
         // right-hand sides of the thread's cells: all rows first, so that their independent
@@ -285,16 +389,16 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
             if (EDGE && k == 1 && g.top_edge)
                 dwz = (4.0 * RW_(rp, R_RW, 0, 0) - fs.xin[R_RW][nc + 2 * PL]) * tmpz;
             else if (EDGE && k == g.npz && g.bot_edge)
-                dwz = (fs.xin[R_RW][nc - 2 * PL] - 4.0 * RW_(rm, R_RW, 0, 0)) * tmpz;
+                dwz = (fs.xin[R_RW][nc - 2 * PL] - 4.0 * RM_(R_RW)) * tmpz;
             else
-                dwz = (RW_(rp, R_RW, 0, 0) - RW_(rm, R_RW, 0, 0)) * tmpz;
+                dwz = (RW_(rp, R_RW, 0, 0) - RM_(R_RW)) * tmpz;
             fr -= dwz;
 
             double fu = 0.0, fv = 0.0, fw = 0.0, ft = 0.0;
             double b1 = 0.0, b2f = 0.0, b3 = 0.0;  // B fluxes WW1..WW3 (MHD)
             const double dzk = L.dzzdz[k];
             const double U0 = DV_(d0, D_U, 0, 0), V0 = DV_(d0, D_V, 0, 0), W0 = DV_(d0, D_W, 0, 0);
-            const double ri = DV_(d0, D_RI, 0, 0);
+            const double ri = LEAN ? riq[c] : DV_(d0, D_RI, 0, 0);
             const double Uxp = DV_(d0, D_U, 1, 0), Uxm = DV_(d0, D_U, -1, 0);
             const double Uyp = DV_(d0, D_U, 0, 1), Uym = DV_(d0, D_U, 0, -1);
             const double Uzp = DV_(dp, D_U, 0, 0), Uzm = DV_(dm, D_U, 0, 0);
@@ -321,25 +425,25 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
 
                 // ---- buoyancy and pressure, src/fluxes.cpp:126-152 ----
                 fw = ph.grav * RW_(r0, R_RO, 0, 0);
-                fw -= (DV_(dp, D_P, 0, 0) - DV_(dm, D_P, 0, 0)) * tmpz;
-                fv = (DV_(d0, D_P, 0, -1) - DV_(d0, D_P, 0, 1)) * tmpy;
-                fu = (DV_(d0, D_P, -1, 0) - DV_(d0, D_P, 1, 0)) * hx * dx1;
+                fw -= (PP_ - PM_) * tmpz;
+                fv = (P0_(0, -1) - P0_(0, 1)) * tmpy;
+                fu = (P0_(-1, 0) - P0_(1, 0)) * hx * dx1;
 
                 // ---- momentum advection, src/fluxes.cpp:171-224 ----
                 fu -= (RW_(r0, R_RU, 1, 0) * Uxp - RW_(r0, R_RU, -1, 0) * Uxm) * hx * dx1;
                 fu -= (RW_(r0, R_RU, 0, 1) * Vyp - RW_(r0, R_RU, 0, -1) * Vym) * tmpy;
-                fu -= (RW_(rp, R_RU, 0, 0) * Wzp - RW_(rm, R_RU, 0, 0) * Wzm) * tmpz;
+                fu -= (RW_(rp, R_RU, 0, 0) * Wzp - RM_(R_RU) * Wzm) * tmpz;
                 fv -= (RW_(r0, R_RV, 1, 0) * Uxp - RW_(r0, R_RV, -1, 0) * Uxm) * hx * dx1;
                 fv -= (RW_(r0, R_RV, 0, 1) * Vyp - RW_(r0, R_RV, 0, -1) * Vym) * tmpy;
-                fv -= (RW_(rp, R_RV, 0, 0) * Wzp - RW_(rm, R_RV, 0, 0) * Wzm) * tmpz;
+                fv -= (RW_(rp, R_RV, 0, 0) * Wzp - RM_(R_RV) * Wzm) * tmpz;
                 fw -= (RW_(r0, R_RW, 1, 0) * Uxp - RW_(r0, R_RW, -1, 0) * Uxm) * hx * dx1;
                 fw -= (RW_(r0, R_RW, 0, 1) * Vyp - RW_(r0, R_RW, 0, -1) * Vym) * tmpy;
-                fw -= (RW_(rp, R_RW, 0, 0) * Wzp - RW_(rm, R_RW, 0, 0) * Wzm) * tmpz;
+                fw -= (RW_(rp, R_RW, 0, 0) * Wzp - RM_(R_RW) * Wzm) * tmpz;
 
                 // ---- energy advection, src/fluxes.cpp:229-243 ----
                 const double Txp = RW_(r0, R_TT, 1, 0), Txm = RW_(r0, R_TT, -1, 0);
                 const double Typ = RW_(r0, R_TT, 0, 1), Tym = RW_(r0, R_TT, 0, -1);
-                const double Tzp = RW_(rp, R_TT, 0, 0), Tzm = RW_(rm, R_TT, 0, 0);
+                const double Tzp = RW_(rp, R_TT, 0, 0), Tzm = RM_(R_TT);
                 ft = -1.0 * U0 * (Txp - Txm) * hx * dx1;
                 ft -= V0 * (Typ - Tym) * tmpy;
                 ft -= W0 * (Tzp - Tzm) * tmpz;
@@ -594,6 +698,18 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Shape<MHD, TYV>::m
             }
           }
         }
+        if constexpr (LEAN) {  // this plane's own-cell values become the next plane's k-1 values
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+                const int s0 = own0 + c * SX;
+#pragma unroll
+                for (int f = 0; f < 5; ++f) cm[c][f] = RW_(r0, f, 0, 0);
+            }
+        }
+#undef RM_
+#undef P0_
+#undef PP_
+#undef PM_
 #undef RW_
 #undef DV_
     }
@@ -620,6 +736,9 @@ static void launch_one(dim3 grid, const StageMaps& maps, const Geometry& g, cons
     if (!configured) {
         cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
+        // all of the unified L1 as shared memory, so that the resident CTAs fit
+        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         configured = true;
     }
     const dim3 block(TX, TYV / Cells<MHD, STAGE, TYV>::cpt, 1);

@@ -5,6 +5,7 @@ import pytest
 import r3d_b200 as R
 
 B200_SMS = 148  # the plans below are those of a B200
+FP64_HYDRO_CTAS = 3  # resident 128-thread FP64 hydro stage CTAs per SM
 MAG = ["--lmag", "1", "--beta", "10", "--rm", "1", "--ampb", "0.1", "--bfh", "2", "--bzp", "20"]
 
 
@@ -16,7 +17,7 @@ def grid(npx, npy, npz, *extra):
     (grid(504, 504, 512), (62, 8)),                             # short last chunk (8 x 62 + 16)
     (grid(504, 504, 512, "--precision", "fp32bulk"), (63, 8)),    # four FP32 CTAs per SM
     (grid(504, 504, 2048), (64, 8)),                            # > 64 waves: the tail is negligible
-    (grid(504, 504, 64), (16, 8)),
+    (grid(504, 504, 64), (15, 8)),                              # 4 x 15 + 4 estimated shorter than 4 x 16
     (grid(32, 32, 64), (4, 8)),                                 # one partial wave: waves x planes
     (grid(126, 126, 256, *MAG), (12, 6)),                       # 32x6 MHD tiles, two CTAs per SM
     (grid(252, 252, 256, *MAG), (12, 6)),
@@ -42,7 +43,7 @@ def test_hydro_depth_bounds(npx, npy, npz, monkeypatch):
     d = _default_depth(npz)
     assert rows == 8 and 1 <= k <= d
     tiles = -(-npx // 32) * -(-npy // 8)
-    if tiles * -(-npz // d) >= 2 * 148:
+    if tiles * -(-npz // d) >= FP64_HYDRO_CTAS * 148:
         assert k >= (3 * d + 3) // 4
         assert -(-npz // k) <= -(-npz // d) + 1
     else:
