@@ -331,14 +331,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
 #pragma unroll
             for (int c = 0; c < CPT; ++c) riq[c] = rin[c];
         }
-        if (!derive(k + 1)) s_abort = 1;
-        __syncthreads();
-        if (s_abort) break;
-        if (tid == 0 && k + 2 <= ke + 1) {
-            fence_proxy_async();
-            issue(k + 2);
-        }
-        if constexpr (ZL2) {  // this plane's accumulators, from L2, consumed by the stage update
+        if constexpr (ZL2) {  // this plane's accumulators, from L2, issued before the derive phase and the barrier, consumed by the stage update
 #pragma unroll
             for (int c = 0; c < CPT; ++c) {
 #pragma unroll
@@ -348,6 +341,13 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
                     for (int f = 0; f < NF; ++f) zq[c][f] = fs.z[f][k * PL + colv[c]];
                 }
             }
+        }
+        if (!derive(k + 1)) s_abort = 1;
+        __syncthreads();
+        if (s_abort) break;
+        if (tid == 0 && k + 2 <= ke + 1) {
+            fence_proxy_async();
+            issue(k + 2);
         }
         const double* rm = raw + ((q + NRAW - 1) % NRAW) * S::raw_slot;
         const double* r0 = raw + (q % NRAW) * S::raw_slot;
