@@ -314,9 +314,10 @@ def fp32_error_run(R, local, grid, steps, flags=(), seed=None):
 PLUME = ["--tp", "2", "--tc", "0", "--xp", "10", "--yp", "10", "--zp", "0", "--hh", "1"]
 
 
-def adjoint_run(R, local):
-    """Time of the discrete adjoint on the MHD 64x64x128 case: record 200 steps with a
-    checkpoint every 20, then the checkpointed reverse sweep (seed: d(kinetic energy)/dX).
+def adjoint_run(R, local, steps=200, every=20):
+    """Time of the discrete adjoint on the MHD 64x64x128 case: record `steps` steps with a
+    checkpoint every `every` (200 and 20 by default), then the checkpointed reverse sweep (seed:
+    d(kinetic energy)/dX).
     CUDA events on the library's stream bracket each call (device time, host gaps included);
     the wall clock around the synchronous calls is reported beside them."""
     import numpy as np
@@ -338,7 +339,7 @@ def adjoint_run(R, local):
         torch.cuda.synchronize(local)
         t0 = time.perf_counter()
         ev[0].record(stream)
-        sim.adjoint_record(200, 20)
+        sim.adjoint_record(steps, every)
         ev[1].record(stream)
         t1 = time.perf_counter()
         sim.download(fin)
@@ -356,10 +357,10 @@ def adjoint_run(R, local):
         fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
         mem = sim.adjoint_memory_bytes
     cells = 64 * 64 * 128
-    return {"grid": [64, 64, 128], "steps": 200, "checkpoint_every": 20,
+    return {"grid": [64, 64, 128], "steps": steps, "checkpoint_every": every,
             "forward_record_ms": fwd_ms, "backward_ms": bwd_ms, "backward_over_forward": bwd_ms / fwd_ms,
             "wall_ms": {"forward_record": (t1 - t0) * 1e3, "backward": (t3 - t2) * 1e3},
-            "adjoint_mcell_steps_per_s": cells * 200 / (bwd_ms / 1e3) / 1e6, "adjoint_device_bytes": mem,
+            "adjoint_mcell_steps_per_s": cells * steps / (bwd_ms / 1e3) / 1e6, "adjoint_device_bytes": mem,
             "note": "CUDA events on the library stream around each synchronous C ABI call (the "
                     "backward includes its seed upload and gradient download); wall_ms: host clock"}
 
@@ -451,9 +452,16 @@ def main():
                     help="with --fp32-error: plume forcing tp=2 tc=0 xp=yp=10 zp=0 hh=1, seed 11")
     ap.add_argument("--dry-launch", action="store_true",
                     help="start and join the ranks (gloo) and report them, without GPU work")
+    ap.add_argument("--adjoint", type=int, nargs=2, metavar=("STEPS", "EVERY"),
+                    help="only the adjoint leg (MHD 64x64x128), STEPS recorded with a checkpoint every EVERY")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return spawn_ranks(args.gpus)
+    if args.adjoint:
+        import r3d_b200 as R
+
+        emit(adjoint_run(R, 0, *args.adjoint))
+        return 0
     if args.fp32_error:
         import r3d_b200 as R
 
