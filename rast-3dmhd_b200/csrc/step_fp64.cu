@@ -71,10 +71,11 @@ constexpr int NDER = 4;
 // the derived ring (1/rho of the thread's own cells stays in registers; P = rho*T is formed
 // where it is used, the product the reference stores).  MHD keeps the 4-slot raw ring and the
 // derived u, v, w, P, 1/rho.  Both prefetch the RK accumulators of the next plane into L2 and
-// load a plane's accumulators when its computation starts, which takes fewer registers than
-// holding the next plane's values in registers (hydro: 40; measured on B200 at 1965 MHz:
-// 504x504x512 hydro 15.45 -> 15.06 ms per step, 126x126x256 MHD 0.946 -> 0.901 ms; a prefetch
-// two planes ahead: hydro 15.2-15.3 ms).
+// load a plane's accumulators during the plane - hydro after its fluxes, just before the stage
+// update, MHD before its derive phase - which takes fewer registers than holding the next
+// plane's values in registers (hydro: 40, and no spills).  Measured on B200 at 1965 MHz:
+// 504x504x512 hydro 15.45 -> 14.9 ms per step, 126x126x256 MHD 0.946 -> 0.901 ms (0.936 with
+// the hydro placement); a prefetch two planes ahead was slower in every placement.
 template <bool MHD>
 struct Ring {
     static constexpr bool lean = !MHD;
@@ -264,6 +265,8 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
             for (int c = 0; c < CPT; ++c)
 #pragma unroll
                 for (int f = 0; f < 5; ++f) cm[c][f] = raw[f * RAWF + own0 + c * SX];  // slot 0: plane kb-1
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) cm[c][R_RO] = cm[c][R_RO] * cm[c][R_TT];  // P of plane kb-1
         }
     }
     ok = derive(kb) && ok;
@@ -331,7 +334,8 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
 #pragma unroll
             for (int c = 0; c < CPT; ++c) riq[c] = rin[c];
         }
-        if constexpr (ZL2) {  // this plane's accumulators, from L2, issued before the derive phase and the barrier, consumed by the stage update
+        if constexpr (ZL2 && !LEAN) {
+            // MHD: this plane's accumulators, issued before the derive phase and the barrier
 #pragma unroll
             for (int c = 0; c < CPT; ++c) {
 #pragma unroll
@@ -361,7 +365,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
 #define RM_(F) (LEAN ? cm[c][F] : RW_(rm, F, 0, 0))
 #define P0_(DX, DY) (LEAN ? RW_(r0, R_RO, DX, DY) * RW_(r0, R_TT, DX, DY) : DV_(d0, D_P, DX, DY))
 #define PP_ (LEAN ? RW_(rp, R_RO, 0, 0) * RW_(rp, R_TT, 0, 0) : DV_(dp, D_P, 0, 0))
-#define PM_ (LEAN ? cm[c][R_RO] * cm[c][R_TT] : DV_(dm, D_P, 0, 0))
+#define PM_ (LEAN ? cm[c][R_RO] : DV_(dm, D_P, 0, 0))  // lean: cm[.][R_RO] carries P
         const double tmpz = L.tmpz[k];
         const bool edge = (k == 1 && g.top_edge) || (k == g.npz && g.bot_edge);
         // right-hand sides of the thread's cells: all rows first, so that their independent
@@ -646,6 +650,20 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
                 rhs(EdgeTag<true>{});
             }
         }
+        if constexpr (ZL2 && LEAN) {
+            // hydro: this plane's accumulators (prefetched into L2 a plane earlier), loaded after
+            // the fluxes; the compiler barrier keeps the loads from being hoisted into them
+            asm volatile("" ::: "memory");
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+#pragma unroll
+                for (int f = 0; f < NF; ++f) zq[c][f] = 0.0;
+                if (STAGE > 0 && actv[c]) {
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) zq[c][f] = fs.z[f][k * PL + colv[c]];
+                }
+            }
+        }
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
           if (actv[c]) {
@@ -704,6 +722,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
                 const int s0 = own0 + c * SX;
 #pragma unroll
                 for (int f = 0; f < 5; ++f) cm[c][f] = RW_(r0, f, 0, 0);
+                cm[c][R_RO] = RW_(r0, R_RO, 0, 0) * RW_(r0, R_TT, 0, 0);  // the plane's own P
             }
         }
 #undef RM_
