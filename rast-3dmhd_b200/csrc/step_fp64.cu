@@ -81,7 +81,6 @@ struct Ring {
     static constexpr bool lean = !MHD;
     static constexpr int nraw = lean ? 3 : 4;
     static constexpr int nder_f = lean ? 3 : D_NF;  // derived fields per slot
-    static constexpr bool z_l2 = true;
 };
 
 // Cells per thread: a hydro thread computes CPT adjacent rows of its tile column, so each warp
@@ -175,7 +174,6 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
     const int i = i0 + tx, jr = j0 + ty * CPT;  // the thread's column and first row
 
     constexpr bool LEAN = Ring<MHD>::lean;
-    constexpr bool ZL2 = Ring<MHD>::z_l2;
     constexpr int NRAW = Ring<MHD>::nraw;
     // the thread's own cells in the halo tile (row c of the thread: halo row ty*CPT + c + 1)
     const int own0 = (ty * CPT + 1) * SX + tx + 1;
@@ -284,11 +282,9 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
     // offsets from a cell to its periodic ghost images (0: none)
     const int gdx = (i == 1) ? g.npx : ((i == g.npx) ? -g.npx : 0);
 
-    // per row c of the thread: activity, y metrics, column offset, and the RK accumulator Z of
-    // the cell, loaded one plane ahead (registers)
+    // per row c of the thread: activity, y metrics, column offset
     bool actv[CPT];
     int colv[CPT];
-    double zn[CPT][NF];
     double dxyv[CPT];  // third stage: min(ddx[i], ddy[j]), the plane-independent part of dd
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
@@ -299,30 +295,14 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
             const int ja = (j <= g.npy) ? j : 1;
             dxyv[c] = (L.ddy[ja] < L.ddx[ia]) ? L.ddy[ja] : L.ddx[ia];
         }
-#pragma unroll
-        for (int f = 0; f < NF; ++f) zn[c][f] = 0.0;
-        if (STAGE > 0 && actv[c] && !ZL2) {
-#pragma unroll
-            for (int f = 0; f < NF; ++f) zn[c][f] = fs.z[f][kb * PL + colv[c]];
-        }
     }
 
     for (int k = kb; k <= ke; ++k) {
         const int q = k - (kb - 1);
-        // the next plane's accumulators: issued before the derive phase and the barrier, so
-        // their latency hides behind a whole plane of work
+        // the RK accumulators Z of the thread's cells: the next plane's into L2, this plane's
+        // (zq) loaded below
         double zq[CPT][NF];
-        if constexpr (!ZL2) {
-#pragma unroll
-            for (int c = 0; c < CPT; ++c) {
-#pragma unroll
-                for (int f = 0; f < NF; ++f) zq[c][f] = zn[c][f];
-                if (STAGE > 0 && actv[c] && k < ke) {
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) zn[c][f] = fs.z[f][(k + 1) * PL + colv[c]];
-                }
-            }
-        } else if (STAGE > 0 && k + R3D_ZAHEAD <= ke) {
+        if (STAGE > 0 && k + R3D_ZAHEAD <= ke) {
 #pragma unroll
             for (int c = 0; c < CPT; ++c)
                 if (actv[c]) {
@@ -334,7 +314,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
 #pragma unroll
             for (int c = 0; c < CPT; ++c) riq[c] = rin[c];
         }
-        if constexpr (ZL2 && !LEAN) {
+        if constexpr (!LEAN) {
             // MHD: this plane's accumulators, issued before the derive phase and the barrier
 #pragma unroll
             for (int c = 0; c < CPT; ++c) {
@@ -650,7 +630,7 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
                 rhs(EdgeTag<true>{});
             }
         }
-        if constexpr (ZL2 && LEAN) {
+        if constexpr (LEAN) {
             // hydro: this plane's accumulators (prefetched into L2 a plane earlier), loaded after
             // the fluxes; the compiler barrier keeps the loads from being hoisted into them
             asm volatile("" ::: "memory");
