@@ -85,8 +85,9 @@ struct Ring {
 
 // Cells per thread: a hydro thread computes CPT adjacent rows of its tile column, so each warp
 // carries CPT independent stencil evaluations (and shares the y-neighbour loads between them).
-// Two rows in the first two stages, one in the third (its filtered dt epilogue branches per
-// cell); an MHD cell already needs most of the register file, so MHD threads take one row.
+// Two rows in all three stages (at three CTAs per SM; with one row, 256-thread CTAs, the third
+// stage was 2.5% slower); an MHD cell already needs most of the register file, so MHD threads
+// take one row.
 // The right-hand side's variant of a plane: interior, or a domain edge (one-sided continuity
 // and B stencils; the momentum and energy fluxes, which BCON rewrites, not formed) - or, with
 // FULL, the top edge whose temperature BCON leaves alone (itcon 3): one-sided continuity and
@@ -254,8 +255,9 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
         issue(kb + 1);
     }
     bool ok = derive(kb - 1);
-    // lean layout: the own cells' values of the plane above the chunk (rho, T and the momenta,
-    // the k-1 neighbours of its first plane), carried in registers from plane to plane
+    // lean layout: the own cells' values of the plane above (the momenta, T, and P = rho*T in
+    // the rho slot: the k-1 neighbours of the plane computed), carried in registers from plane
+    // to plane
     double cm[CPT][5];
     if constexpr (LEAN) {
         if (ok) {
