@@ -372,9 +372,31 @@ def reference_layout(ncores: int):
     return ranks, max(1, ncores // ranks)
 
 
+REF_BUDGET_S = 300.0  # wall time the reference arm's W + K steps may take (60 + 3 full steps: ~285 s)
+
+
+def reference_depth(ranks: int, threads: int, steps: int) -> int:
+    """Planes of the reference arm's grid: all of the benchmark grid's when W + K of its steps
+    fit REF_BUDGET_S (R3D_REF_BUDGET_S overrides) on this host, else the depth that does (a
+    bounded sample of the same planes; at least 32).  The per-plane cost comes from one timed
+    step on 32 planes of the grid."""
+    from oracle import Reference
+
+    budget = float(os.environ.get("R3D_REF_BUDGET_S", REF_BUDGET_S))
+    cal_depth = min(32, GRID[2])
+    cal = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(cal_depth), "--npey", "1"]
+    _, sec = Reference.time_steps(cal, ranks, SEED, 0, 1, threads)
+    per_plane = sec / cal_depth
+    if steps * per_plane * GRID[2] <= budget:
+        return GRID[2]
+    return min(GRID[2], max(32, int(budget / (steps * per_plane)) // 8 * 8))
+
+
 def run_reference_arm(args, world, rank, pg):
     """The reference's own CPU implementation (src/*.cpp compiled unmodified, thread-rank MPI
-    stand-in, OpenMP) on the benchmark grid: set-up, W untimed steps, K timed steps."""
+    stand-in, OpenMP): set-up, W untimed steps, K timed steps on the benchmark grid, or on a
+    shallower grid of the same planes when W + K full steps would take more than a few minutes
+    (reference_depth)."""
     if rank != 0:
         return 0
     base = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
@@ -387,19 +409,22 @@ def run_reference_arm(args, world, rank, pg):
                   "unavailable": "reference CPU build oracle/_ref/libr3dref.so not present"})
             return 0
         ncores = os.cpu_count() or 1
-        fl = FLAGS + ["--npey", "1"]
-        cells = GRID[0] * GRID[1] * GRID[2]
         ranks, threads = reference_layout(ncores)
+        depth = reference_depth(ranks, threads, args.warmup + args.steps)
+        fl = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(depth), "--npey", "1"]
+        cells = GRID[0] * GRID[1] * depth
         sc, sec = Reference.time_steps(fl, ranks, SEED, args.warmup, args.steps, threads)
         v = cells * args.steps / sec / 1e6
+        what = ("the full benchmark grid" if depth == GRID[2] and world == 1 else
+                f"a bounded sample of the {GRID[0]}x{GRID[1]}x{GRID[2] * world} workload: {depth} of its planes")
         sample = (f"reference CPU sources compiled unmodified (-O2 -ffp-contract=off -fopenmp), "
                   f"{ranks} thread-ranks x {threads} OpenMP threads on {ncores} host threads, grid "
-                  f"{GRID[0]}x{GRID[1]}x{GRID[2]} (the full benchmark grid), {args.warmup} untimed + "
+                  f"{GRID[0]}x{GRID[1]}x{depth} ({what}), {args.warmup} untimed + "
                   f"{args.steps} timed RK3 steps, seed {SEED}")
         out = {**base, "value": v, "ms_per_step": sec / args.steps * 1e3, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": f"FP64 hydro {GRID[0]}x{GRID[1]}x{GRID[2]} default physics seed {SEED}",
-                          "grid": list(GRID)},
+               "config": {"workload": f"FP64 hydro {GRID[0]}x{GRID[1]}x{GRID[2] * world} default physics seed {SEED}",
+                          "grid": [GRID[0], GRID[1], GRID[2] * world], "sampled_grid": [GRID[0], GRID[1], depth]},
                "final_dt": sc["dt"],
                "cpu_baseline": {"value": v, "unit": UNIT, "cores": ranks * threads, "kind": "reference",
                                 "sample": sample},

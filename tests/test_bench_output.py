@@ -28,6 +28,22 @@ def test_reference_arm_prints_one_json_line():
     assert out["cpu_baseline"]["kind"] == "reference" and out["cpu_baseline"]["cores"] >= 1
     assert out["e2e"]["h2d_bytes_per_step"] == 0
     assert out["config"]["grid"] == [48, 32, 16] and out["steps"] == 1 and out["warmup"] == 3
+    assert out["config"]["sampled_grid"] == [48, 32, 16] and "full benchmark grid" in out["cpu_baseline"]["sample"]
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libr3dref.so")),
+                    reason="reference CPU build not present")
+def test_reference_arm_samples_planes_when_the_run_would_be_long():
+    """W + K full-grid reference steps that would exceed the arm's time budget run on fewer of
+    the grid's planes (at least 32), and the line says so."""
+    env = dict(os.environ, R3D_REF_BUDGET_S="0.001")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--grid", "48", "32", "64"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = json.loads([ln for ln in r.stdout.splitlines() if ln.strip()][0])
+    assert out["config"]["grid"] == [48, 32, 64] and out["config"]["sampled_grid"] == [48, 32, 32]
+    assert "bounded sample" in out["cpu_baseline"]["sample"] and out["value"] > 0
 
 
 @pytest.mark.parametrize("n", [2, 3])
