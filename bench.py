@@ -372,24 +372,30 @@ def reference_layout(ncores: int):
     return ranks, max(1, ncores // ranks)
 
 
-REF_BUDGET_S = 300.0  # wall time the reference arm's W + K steps may take (60 + 3 full steps: ~285 s)
+REF_BUDGET_S = 330.0  # wall time the reference arm's W + K steps may take (3 + 60 full steps: ~290 s)
 
 
 def reference_depth(ranks: int, threads: int, steps: int) -> int:
     """Planes of the reference arm's grid: all of the benchmark grid's when W + K of its steps
     fit REF_BUDGET_S (R3D_REF_BUDGET_S overrides) on this host, else the depth that does (a
-    bounded sample of the same planes; at least 32).  The per-plane cost comes from one timed
-    step on 32 planes of the grid."""
+    bounded sample of the same planes; at least 32).  The step time is modelled as a + b *
+    planes from one timed step on 32 and one on 64 planes of the grid."""
     from oracle import Reference
 
     budget = float(os.environ.get("R3D_REF_BUDGET_S", REF_BUDGET_S))
-    cal_depth = min(32, GRID[2])
-    cal = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(cal_depth), "--npey", "1"]
-    _, sec = Reference.time_steps(cal, ranks, SEED, 0, 1, threads)
-    per_plane = sec / cal_depth
-    if steps * per_plane * GRID[2] <= budget:
+    if GRID[2] <= 32:
         return GRID[2]
-    return min(GRID[2], max(32, int(budget / (steps * per_plane)) // 8 * 8))
+
+    def one_step(depth):
+        fl = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(depth), "--npey", "1"]
+        return Reference.time_steps(fl, ranks, SEED, 0, 1, threads)[1]
+
+    t32, t64 = one_step(32), one_step(64)
+    b = max((t64 - t32) / 32, 1e-9)
+    a = max(t32 - 32 * b, 0.0)
+    if steps * (a + b * GRID[2]) <= budget:
+        return GRID[2]
+    return min(GRID[2], max(32, int((budget / steps - a) / b) // 8 * 8))
 
 
 def run_reference_arm(args, world, rank, pg):
