@@ -309,7 +309,7 @@ def fp32_error_run(R, local, grid, steps, flags=(), seed=None):
     return out
 
 
-# FP32-bulk 504 x 504 x 2048 with the reference's plume top boundary
+# The plume workload: FP32-bulk 504 x 504 x 2048 with the reference's plume top boundary
 # (tp 2, itcon 1; src/bcon.cpp:43-70), seed 11, 50 steps, FP64 alongside
 PLUME = ["--tp", "2", "--tc", "0", "--xp", "10", "--yp", "10", "--zp", "0", "--hh", "1"]
 
@@ -621,7 +621,7 @@ def main():
                                                  max(args.steps, 20), args.warmup, 640.0, None)
         extra["adjoint_mhd_64x64x128"] = adjoint_run(R, local)
         extra["fp32bulk_error_504x504x512_100steps"] = fp32_error_run(R, local, GRID, 100)
-        extra["config4_fp32bulk_plume_504x504x2048_50steps"] = fp32_error_run(R, local, (504, 504, 2048), 50,
+        extra["fp32bulk_plume_504x504x2048_50steps"] = fp32_error_run(R, local, (504, 504, 2048), 50,
                                                                               PLUME, seed=11)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:

@@ -105,7 +105,7 @@ def test_device_compare_equals_host_norms():
 
 
 @pytest.mark.gpu
-def test_config4_plume_504x504x2048_fp32bulk_vs_fp64():
+def test_plume_504x504x2048_fp32bulk_vs_fp64():
     """The FP32-bulk benchmark configuration: 504 x 504 x 2048 with the reference's plume top
     boundary (tp 2, itcon 1, Gaussian at xp = yp = 10, zp 0, hh 1; src/bcon.cpp:43-70), seed 11,
     50 steps, the FP64 form alongside from the same initial state (63 + 32 GB on the device, built
