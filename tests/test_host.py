@@ -83,7 +83,7 @@ def test_parser_rejects_unknown_and_missing_values():
     (["--npz", "4"], "too small"),
 ])
 def test_unsupported_configurations_are_errors(args, msg):
-    """Configurations this build refuses, with the reason (ITCON 2 and 3 run in the fp64 form)."""
+    """Configurations the library refuses, with the reason (ITCON 2 and 3 run in the fp64 form)."""
     with pytest.raises(R.R3dError) as e:
         R.check(R.parse(args))
     assert e.value.code == R.R3D_EINVAL and msg in str(e.value)
