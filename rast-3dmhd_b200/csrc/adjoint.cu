@@ -84,10 +84,13 @@ __global__ void __launch_bounds__(BX* BY) adj_seed_kernel(AdjArgs A, double* lam
     if (i <= A.g.npx && j <= A.g.npy) {
         const int n = k * (int)A.g.plane + j * (int)A.g.pitch + i;
         const double gdt = gam * A.sc->dt;
-        for (int f = 0; f < A.nf; ++f) {
-            const double ly = A.lam[f][n];
-            lf[f][n] = (first ? 0.0 : lf[f][n]) + gdt * ly;
-            dot += A.fprev[f][n] * ly;  // fprev carries F_s here
+#pragma unroll
+        for (int f = 0; f < 8; ++f) {  // unrolled: the pointer table stays in registers
+            if (f < A.nf) {
+                const double ly = A.lam[f][n];
+                lf[f][n] = (first ? 0.0 : lf[f][n]) + gdt * ly;
+                dot += A.fprev[f][n] * ly;  // fprev carries F_s here
+            }
         }
     }
     block_sum_store(dot, dots);

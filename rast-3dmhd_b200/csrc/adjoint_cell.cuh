@@ -284,16 +284,13 @@ R3D_HD double adj_pass2_cell(const AdjArgs& A, int i, int j, int k) {
         if (k >= 2 && k <= npz - 1) s -= 2.0 * L.tmpz2[k] * F[n];
         if (k - 1 >= 2 && k - 1 <= npz - 1) s += (L.tmpz1[k - 1] + L.tmpz2[k - 1]) * F[zm];
         if (k + 1 >= 2 && k + 1 <= npz - 1) s += (-L.tmpz1[k + 1] + L.tmpz2[k + 1]) * F[zp];
-        const double l4[4] = {2.0, -5.0, 4.0, -1.0};
+        // coefficients of f(1+o) (top) / f(npz-o) (bottom), o = 0..3, in the one-sided first
+        // (s) and second (l) differences; selected, not indexed, so that no local array is made
+        auto l4 = [](int o) { return o == 0 ? 2.0 : (o == 1 ? -5.0 : (o == 2 ? 4.0 : -1.0)); };
+        auto s4 = [](int o) { return o == 0 ? -3.0 : (o == 1 ? 4.0 : (o == 2 ? -1.0 : 0.0)); };
         const int o1 = k - 1, o2 = npz - k;
-        if (o1 <= 3) {
-            const double s4[4] = {-3.0, 4.0, -1.0, 0.0};
-            s += (L.tmpz1[1] * s4[o1] + L.tmpz2[1] * l4[o1]) * F[c1];
-        }
-        if (o2 <= 3) {
-            const double s4[4] = {3.0, -4.0, 1.0, 0.0};
-            s += (L.tmpz1[npz] * s4[o2] + L.tmpz2[npz] * l4[o2]) * F[c2];
-        }
+        if (o1 <= 3) s += (L.tmpz1[1] * s4(o1) + L.tmpz2[1] * l4(o1)) * F[c1];
+        if (o2 <= 3) s += (L.tmpz1[npz] * -s4(o2) + L.tmpz2[npz] * l4(o2)) * F[c2];
         return s;
     };
     // transposed T stencils (the Lambda already carry their coefficients)
@@ -345,12 +342,15 @@ R3D_HD double adj_pass2_cell(const AdjArgs& A, int i, int j, int k) {
     // receives zeta_s dt lambda_Y
     double dot = 0.0;
     const double zdt = A.zeta * A.sc->dt;
-    for (int f = 0; f < A.nf; ++f) {
-        const double ly_ = A.lam[f][n];
-        A.lam[f][n] = out[f] + ly_;
-        if (A.fnext[0]) {
-            A.fnext[f][n] = zdt * ly_;
-            dot += A.fprev[f][n] * ly_;
+#pragma unroll
+    for (int f = 0; f < kMaxFields; ++f) {  // unrolled over the largest field count: out[] stays in registers
+        if (f < A.nf) {
+            const double ly_ = A.lam[f][n];
+            A.lam[f][n] = out[f] + ly_;
+            if (A.fnext[0]) {
+                A.fnext[f][n] = zdt * ly_;
+                dot += A.fprev[f][n] * ly_;
+            }
         }
     }
     return dot;
