@@ -90,6 +90,23 @@ def test_hydro_steps_bitexact(name, flags, seed, steps):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kchunk", [1, 2, 3, 7])
+@pytest.mark.parametrize("name,flags,seed", [
+    ("ragged_37x13x23", ["--npx", "37", "--npy", "13", "--npz", "23"], 5),
+    ("variable_kappa_itcon3", ["--npx", "24", "--npy", "20", "--npz", "30", "--pzp", "0.5", "--sigma", "0.1",
+                               "--polys", "1.5", "--itcon", "3"], 7),
+], ids=["ragged", "variable_kappa_itcon3"])
+def test_shallow_z_chunks_bitexact(name, flags, seed, kchunk, monkeypatch):
+    """Chunks of 1, 2, 3 and 7 planes (R3D_KCHUNK): every chunk starts from its own plane above
+    and runs the raw ring's first slots, so the ring's start-up, its refill guards and the
+    registers carried from plane to plane are exercised at every depth."""
+    monkeypatch.setenv("R3D_KCHUNK", str(kchunk))
+    st, sc = gpu_run(flags, seed, 4)
+    o = oracle_run(flags, seed, 4)
+    assert_bitexact(st, o, sc)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("stages", [1, 2, 3])
 def test_partial_step_bitexact(stages):
     """step(nstages) for the per-stage bisection the reference tests use
