@@ -6,7 +6,8 @@ Fortran source itself (golden/fortran/3dmhdsub.f, the `IF (LMAG) THEN ... ENDIF`
 SUBROUTINE FLUXES, lines 2146-2651) is read and its statements are executed as written:
 
 * fixed-form lines: comments (c, C, *, ! in column 1) dropped, continuation lines (non-blank,
-  non-zero column 6) joined, statement labels taken from columns 1-5;
+  non-zero column 6, or a leading tab followed by a digit 1-9) joined, statement labels taken
+  from columns 1-5;
 * statements: `DO <label> <var>=<lo>,<hi>` nests closed by `<label> CONTINUE`, assignments to
   arrays or scalars, and `IF (MYPEZ.EQ.0) THEN / ELSE IF (MYPEZ.EQ.NPEZ-1) THEN / ENDIF`;
 * expressions: a recursive-descent parser for + - * / and ** (left to right, unary minus),
@@ -34,7 +35,7 @@ from typing import Dict, List, Tuple
 import numpy as np
 
 ARRAYS_1D = {"DXXDX": 2, "D2XXDX2": 2, "DYYDY": 1, "D2YYDY2": 1, "DZZDZ": 0, "D2ZZDZ2": 0,
-             "EXX": 2, "WYY": 1, "ZEE": 0}
+             "EXX": 2, "WYY": 1, "ZEE": 0, "ROM": 0, "WWZ": 0}
 
 
 def read_block(path: str, first: int = 2146, last: int = 2651) -> List[Tuple[str, str]]:
@@ -44,7 +45,15 @@ def read_block(path: str, first: int = 2146, last: int = 2651) -> List[Tuple[str
     for line in raw:
         if not line.strip() or line[0] in "cC*!":
             continue
-        line = line.expandtabs(8) if not line.startswith("\t") else line
+        if line.startswith("\t"):
+            # tab format: a tab followed by a digit 1-9 continues the statement before, any
+            # other tab-led line is a statement (no label)
+            if len(line) > 1 and line[1] in "123456789":
+                stmts[-1][1] += line[2:].strip()
+                continue
+            stmts.append(["", line.strip()])
+            continue
+        line = line.expandtabs(8)
         if len(line) > 5 and line[:5].strip() == "" and line[5] not in " 0\t":
             stmts[-1][1] += line[6:].strip()
             continue

@@ -65,6 +65,7 @@ class Oracle:
             lib.ora_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.ora_fluxes.argtypes = [ctypes.c_void_p]
             lib.ora_heat_loss.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.ora_density_diffusion.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.ora_communicate.argtypes = [ctypes.c_void_p]
             lib.ora_field.restype = ctypes.POINTER(ctypes.c_double)
             lib.ora_field.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -117,6 +118,13 @@ class Oracle:
         shape (NZ, NY, NX)."""
         out = np.zeros((self.NZ, self.NY, self.NX))
         self._check(self.lib().ora_heat_loss(self.h, out.ctypes.data))
+        return out
+
+    def density_diffusion(self) -> np.ndarray:
+        """The density-diffusion terms (ID 1, 2) of the current state (FR starting from zeros),
+        shape (NZ, NY, NX)."""
+        out = np.zeros((self.NZ, self.NY, self.NX))
+        self._check(self.lib().ora_density_diffusion(self.h, out.ctypes.data))
         return out
 
     def field(self, name: str) -> np.ndarray:

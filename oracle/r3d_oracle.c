@@ -605,6 +605,111 @@ int ora_heat_loss(ora_sim* s, double* ft) {
     return 0;
 }
 
+/* Density diffusion (ID 1 or 2), 3dmhdsub.f:1316-1382, the part of FLUXES after FR's
+   continuity terms: the density ghost planes are loaded with their mirror planes (RO(k=0) =
+   RO(2), RO(NZ-1) = RO(NZ-3); kept in the state, as the Fortran does), ROM(k) is the horizontal
+   mean of every plane (HORIZONTAL_MEAN, 3dmhdsub.f:3160-3186, the uniform grid it requires: the
+   interior (j, i) sum in loop order over FLOAT(NPX*NPY), a single rank in y), WW1 = RO - ROM,
+   and FR receives DH*ORE*WWZ times its x and y second-difference operators and DV*ORE*WWZ times
+   its z one.  WWZ = 1/ROM (ID 1) or exp(CLN*ZEE**2) + exp(CLN*(ZEE-ZMAX)**2) with SGM = 0.1E00
+   and CLN = -4.0E00*LOG(2.0E00)/SGM/SGM (ID 2; single-precision literals as written). */
+static void density_diffusion(ora_sim* s, double* FR) {
+    const ora_params* p = &s->p;
+    const int NX = s->NX, NY = s->NY, NZ = s->NZ;
+    const int i1 = 1, i2 = NX - 2, j1 = 1, j2 = NY - 2, k1 = 1, k2 = NZ - 2;
+    double* RO = s->f[ORA_RO];
+    double *W1 = s->f[ORA_WW1], *W2 = s->f[ORA_WW2], *W3 = s->f[ORA_WW3];
+    const double *dxxdx = s->line[ORA_DXXDX], *d2xxdx2 = s->line[ORA_D2XXDX2];
+    const double *dyydy = s->line[ORA_DYYDY], *d2yydy2 = s->line[ORA_D2YYDY2];
+    const double *dzzdz = s->line[ORA_DZZDZ], *d2zzdz2 = s->line[ORA_D2ZZDZ2], *zee = s->line[ORA_ZEE];
+    const double hx = s->hx, h2x = s->h2x, hy = s->hy, h2y = s->h2y, hz = s->hz, h2z = s->h2z;
+    const long sx = 1, sy = NX, sz = (long)NX * NY;
+    for (int j = 0; j < NY; ++j) for (int i = 0; i < NX; ++i) {
+        RO[IDX(i, j, 0)] = RO[IDX(i, j, 2)];
+        RO[IDX(i, j, NZ - 1)] = RO[IDX(i, j, NZ - 3)];
+    }
+    double* rom = (double*)malloc(sizeof(double) * (size_t)NZ * 2);
+    double* wwz = rom + NZ;
+    const double cnt = F4((float)(p->npx * p->npy));
+    for (int k = 0; k < NZ; ++k) {
+        double sum = 0.0;
+        for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) sum = sum + RO[IDX(i, j, k)];
+        rom[k] = sum / cnt;
+    }
+    for (int k = 0; k < NZ; ++k) for (int j = 0; j < NY; ++j) for (int i = 0; i < NX; ++i) {
+        long n = IDX(i, j, k);
+        W1[n] = RO[n] - rom[k];
+    }
+    if (p->id == 1) {
+        for (int k = 0; k < NZ; ++k) wwz[k] = 1.0 / rom[k];
+    } else {
+        const double sgm = F4(0.1f);
+        const double cln = F4(-4.0f * logf(2.0f)) / sgm / sgm;
+        for (int k = 0; k < NZ; ++k)
+            wwz[k] = exp(cln * (zee[k] * zee[k])) + exp(cln * ((zee[k] - p->zmax) * (zee[k] - p->zmax)));
+    }
+#define A(F, di, dj, dk) F[n + (di) * sx + (dj) * sy + (dk) * sz]
+    if (p->dh != 0.0) {
+        for (int k = k1; k <= k2; ++k) for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) {
+            long n = IDX(i, j, k);
+            W2[n] = (A(W1, 1, 0, 0) - A(W1, -1, 0, 0)) * hx * d2xxdx2[i] +
+                    (A(W1, 1, 0, 0) - 2.0 * W1[n] + A(W1, -1, 0, 0)) * h2x * dxxdx[i] * dxxdx[i];
+        }
+        for (int k = k1; k <= k2; ++k) for (int j = j1; j <= j2; ++j) {
+            const double tmpy1 = hy * d2yydy2[j], tmpy2 = h2y * dyydy[j] * dyydy[j];
+            for (int i = i1; i <= i2; ++i) {
+                long n = IDX(i, j, k);
+                W3[n] = (A(W1, 0, 1, 0) - A(W1, 0, -1, 0)) * tmpy1 +
+                        (A(W1, 0, 1, 0) - 2.0 * W1[n] + A(W1, 0, -1, 0)) * tmpy2;
+            }
+        }
+        for (int k = k1; k <= k2; ++k) {
+            const double tmp = p->dh * s->ore * wwz[k];
+            for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) {
+                long n = IDX(i, j, k);
+                FR[n] = FR[n] + (W2[n] + W3[n]) * tmp;
+            }
+        }
+    }
+    if (p->dv != 0.0) {
+        for (int k = k1; k <= k2; ++k) {
+            const double tmpz1 = hz * d2zzdz2[k], tmpz2 = h2z * dzzdz[k] * dzzdz[k];
+            for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) {
+                long n = IDX(i, j, k);
+                W2[n] = (A(W1, 0, 0, 1) - A(W1, 0, 0, -1)) * tmpz1 +
+                        (A(W1, 0, 0, 1) - 2.0 * W1[n] + A(W1, 0, 0, -1)) * tmpz2;
+            }
+        }
+        for (int k = k1; k <= k2; ++k) {
+            const double tmp = p->dv * s->ore * wwz[k];
+            for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) {
+                long n = IDX(i, j, k);
+                FR[n] = FR[n] + W2[n] * tmp;
+            }
+        }
+    }
+#undef A
+    free(rom);
+}
+
+/* The density-diffusion terms alone (added to fr, normally zeros) for the current state, with
+   rho in RO (its value at the start of FLUXES): the pin of density_diffusion against the
+   Fortran block executed statement by statement.  The state's ghost planes are restored. */
+int ora_density_diffusion(ora_sim* s, double* fr) {
+    if (s->p.id != 1 && s->p.id != 2) { set_err("ID must be 1 or 2"); return -1; }
+    const long plane = (long)s->NX * s->NY;
+    double* RO = s->f[ORA_RO];
+    double* keep = (double*)malloc(sizeof(double) * (size_t)plane * 2);
+    if (!keep) { set_err("out of memory"); return -1; }
+    memcpy(keep, RO, sizeof(double) * (size_t)plane);
+    memcpy(keep + plane, RO + (s->NZ - 1) * plane, sizeof(double) * (size_t)plane);
+    density_diffusion(s, fr);
+    memcpy(RO, keep, sizeof(double) * (size_t)plane);
+    memcpy(RO + (s->NZ - 1) * plane, keep + plane, sizeof(double) * (size_t)plane);
+    free(keep);
+    return 0;
+}
+
 static void fluxes(ora_sim* s) {
     const ora_params* p = &s->p;
     const int NX = s->NX, NY = s->NY, NZ = s->NZ;
@@ -639,6 +744,7 @@ static void fluxes(ora_sim* s) {
       for (int j = j1; j <= j2; ++j) for (int i = i1; i <= i2; ++i) { long n = IDX(i, j, k2);
           W1[n] = (A(RW, 0, 0, -2) - 4.0 * A(RW, 0, 0, -1)) * tmpz; } }
     OMP LOOP_INT { long n = IDX(i, j, k); FR[n] -= W1[n]; }
+    if (p->id != 0) density_diffusion(s, FR);
 
     /* buoyancy, pressure, 1/rho, velocities: src/fluxes.cpp:126-166 */
     OMP LOOP_INT { long n = IDX(i, j, k); FW[n] = p->grav * RO[n]; }
@@ -955,7 +1061,7 @@ static int bcon(ora_sim* s) {
 /* src/step.cpp:114-257 (+ B terms of 3dmhdsub.f STEP when lmag). */
 int ora_step(ora_sim* s, int nstages) {
     const ora_params* p = &s->p;
-    if (p->lshr || p->lrem || p->rlax > 0.0 || p->id != 0 ||
+    if (p->lshr || p->lrem || p->rlax > 0.0 || (p->id != 0 && (p->ngrid != 0 || (p->id != 1 && p->id != 2))) ||
         p->ixcon != 0 || p->iycon != 0) { set_err("unsupported FLUXES feature"); return -1; }
     const int NX = s->NX, NY = s->NY, NZ = s->NZ;
     const int i1 = 1, i2 = NX - 2, j1 = 1, j2 = NY - 2, k1 = 1, k2 = NZ - 2;

@@ -59,6 +59,8 @@ int ora_param(const ora_sim* s, const char* name, double* out);
 /* The itcon-2 embedded heat-loss term of the current state added to ft (test of the
    restatement against the Fortran block). */
 int ora_heat_loss(ora_sim* s, double* ft);
+/* density-diffusion terms (ID 1, 2) of the current state added to fr */
+int ora_density_diffusion(ora_sim* s, double* fr);
 
 #ifdef __cplusplus
 }
