@@ -253,6 +253,7 @@ dim3 cell_grid(const r3d_gpu* g) {
 Adjoint* workspace(r3d_gpu* g) {
     if (g->adj) return g->adj;
     if (g->fp32) throw Error(R3D_EINVAL, "the adjoint is available for precision fp64 only");
+    if (g->p.id != 0) throw Error(R3D_EINVAL, "the adjoint does not include the density diffusion (ID)");
     if (g->p.itcon == 2 || g->p.itcon == 3)
         throw Error(R3D_EINVAL, "the adjoint covers itcon 0, 1 and 4 (not the embedded heat loss or a free top T)");
     if (g->nloc != g->p.npz || g->halo) throw Error(R3D_EINVAL, "the adjoint needs the whole domain on one handle");

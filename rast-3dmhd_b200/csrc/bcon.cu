@@ -101,6 +101,39 @@ __global__ void __launch_bounds__(256) bcon_kernel(Geometry g, Physics ph, Lines
     if (with_dt) reduce_dt(red, m1, m2, m3, m4, mu, sc);
 }
 
+// ---------------------------------------------------------------------------------------
+// Horizontal mean of rho per plane for the density diffusion (ID 1, 2): HORIZONTAL_MEAN of the
+// Fortran (3dmhdsub.f:3177-3186, the uniform grid it requires, one rank in y): the plane's
+// interior values added in loop order (j outer, i inner) and divided by FLOAT(NPX*NPY).  One
+// thread per plane keeps that order exactly.  The domain's ghost planes are first loaded with
+// their mirror planes (3dmhdsub.f:1318, 1321), so their means are those of planes 2 and npz-1.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) plane_mean_kernel(Geometry g, const double* ro, double* rom, double* wwz,
+                                                          int id_mode) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > g.npz + 1) return;
+    int src = k;
+    if (k == 0 && g.top_edge) src = 2;
+    if (k == g.npz + 1 && g.bot_edge) src = g.npz - 1;
+    const double* p = ro + (int64_t)src * g.plane;
+    double sum = 0.0;
+    for (int j = 1; j <= g.npy; ++j) {
+        const double* r = p + (int64_t)j * g.pitch;
+#pragma unroll 8
+        for (int i = 1; i <= g.npx; ++i) sum = sum + r[i];
+    }
+    const double m = sum / (double)(float)(g.npx * g.npy);
+    rom[k] = m;
+    if (id_mode == 1) wwz[k] = 1.0 / m;  // WWZ = 1.0E00/ROM (3dmhdsub.f:1338)
+}
+
+cudaError_t launch_plane_mean(const Geometry& g, const double* ro, double* rom, double* wwz, int id_mode,
+                              cudaStream_t st) {
+    const int n = g.npz + 2;
+    plane_mean_kernel<<<(n + 127) / 128, 128, 0, st>>>(g, ro, rom, wwz, id_mode);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_bcon(const Geometry& g, const Physics& ph, const Lines& L, const Boundary& b,
                         const FieldSet& fs, Scalars* sc, int with_dt, cudaStream_t st) {
     dim3 block(32, 8, 1);

@@ -42,6 +42,10 @@ struct Physics {
     int heat_on, hh_one;  // hh_one: HH == 1, where x/HH == x (the divisions are skipped)
     int top_free;         // itcon 3: BCON leaves the top temperature; its flux is formed there
     double heat_pre, hh;
+    // density diffusion (ID 1, 2; 3dmhdsub.f:1316-1386): FR += (d2x + d2y)(rho - rom) * dh_ore*wwz
+    // + d2z(rho - rom) * dv_ore*wwz, rom the horizontal mean of rho per plane
+    int id_mode;
+    double id_dh, id_dv, id_dh_ore, id_dv_ore;  // DH, DV and DH*ORE, DV*ORE
     float gamma_f, ogamma_f, obeta_f;  // float copies for the estimates of the dt filter
 };
 
@@ -54,6 +58,9 @@ struct Lines {
     const double *plume_x, *plume_y;                          // [npx+2], [npy+2]
     // embedded heat loss (itcon 2): exp(CLN*(x - xp)^2) etc. per line, CLN = f4(-4 ln 2)/HH/HH
     const double *heat_x, *heat_y, *heat_z;                   // [npx+2], [npy+2], [npz+2]
+    // density diffusion: the horizontal mean of rho per plane of the stage's input (written by
+    // plane_mean_kernel before each stage) and the vertical profile WWZ   [npz+2] each
+    const double *rom, *wwz;
 };
 
 // Error codes stored in Scalars::err by kernels that abandon a bounded wait.

@@ -391,6 +391,14 @@ void launch_dt_full_any(r3d_gpu* g, int only_refold) {
                 "dt_full");
 }
 
+// Density diffusion: the horizontal means of rho (and WWZ for ID 1) of the stage's input state,
+// into the line buffer the stage kernel reads them from.
+void launch_plane_mean(r3d_gpu* g, const FieldSet& fs) {
+    cuda_ok(r3dk::launch_plane_mean(g->geo, fs.xin[3], const_cast<double*>(g->lines.rom),
+                                    const_cast<double*>(g->lines.wwz), g->ph.id_mode, g->stream),
+            "plane_mean");
+}
+
 // Queue one step (nstages substages) on the device.
 void enqueue_step_begin(r3d_gpu* g) {
     Range r("r3d.step_begin");
@@ -411,6 +419,7 @@ void enqueue_stage(r3d_gpu* g, int s) {
                 "bcon32");
     } else {
         FieldSet fs = fieldset(g);
+        if (g->ph.id_mode) launch_plane_mean(g, fs);
         cuda_ok(r3dk::launch_stage_fp64(s, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream),
                 "stage");
         cuda_ok(r3dk::launch_bcon(g->geo, g->ph, g->lines, g->bnd, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon");
@@ -447,6 +456,12 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
             cuda_ok(r3dk::launch_bcon_fp32(g->geo, g->ph, g->lines, g->bnd, g->bg, fs, g->dsc, s == 2 ? 1 : 0, g->stream), "bcon32");
         } else {
             FieldSet fs = fieldset(g);
+            if (g->ph.id_mode) {
+                launch_plane_mean(g, fs);
+                tm.end(2);
+                ++launches;
+                tm.begin();
+            }
             cuda_ok(r3dk::launch_stage_fp64(s, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream), "stage");
             tm.end(0);
             tm.begin();
@@ -641,11 +656,24 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
             hz_[k] = std::exp(clh * (a * a));
         }
     }
+    // density diffusion (ID 1, 2; 3dmhdsub.f:1337-1344): the per-plane horizontal means of rho
+    // (written on the device before each stage) and WWZ, for ID 2 the Fortran's
+    // EXP(CLN*ZEE**2)+EXP(CLN*(ZEE-ZMAX)**2) with SGM=0.1E00, CLN=-4.0E00*LOG(2.0E00)/SGM/SGM
+    // (single-precision literals); host libm.  ID 1: WWZ = 1/ROM, written with the means.
+    std::vector<double> rom_(NZ, 0.0), wwz_(NZ, 0.0);
+    if (p.id == 2) {
+        const double sgm = (double)0.1f;
+        const double cln = (double)(-4.0f * logf(2.0f)) / sgm / sgm;
+        for (int64_t k = 0; k < NZ; ++k) {
+            const double z = st->zee[k], zm = st->zee[k] - p.zmax;
+            wwz_[k] = std::exp(cln * (z * z)) + std::exp(cln * (zm * zm));
+        }
+    }
     std::vector<const std::vector<double>*> tabs = {&dxxdx, &d2xxdx2, &ddx,  &dyydy, &tmpy,
                                                     &tmpy1, &tmpy2,   &ddy,  &dzzdz, &d2zzdz2,
                                                     &tmpz,  &tmpz1,   &tmpz2, &ddz,  &rkapa,
                                                     &dkapa, &px,      &py,   &d2yydy2, &hx_,
-                                                    &hy_,   &hz_};
+                                                    &hy_,   &hz_,     &rom_, &wwz_};
     size_t total = 0;
     for (auto* t : tabs) total += (t->size() + 15) / 16 * 16;
     if (!g->line_buf) {
@@ -669,6 +697,12 @@ void upload_lines(r3d_gpu* g, const r3d_host_state* st) {
     L.ddz = dev[13]; L.rkapa = dev[14]; L.dkapa = dev[15]; L.plume_x = dev[16]; L.plume_y = dev[17];
     L.d2yydy2 = dev[18];
     L.heat_x = dev[19]; L.heat_y = dev[20]; L.heat_z = dev[21];
+    L.rom = dev[22]; L.wwz = dev[23];
+    g->ph.id_mode = p.id;
+    g->ph.id_dh = p.dh;
+    g->ph.id_dv = p.dv;
+    g->ph.id_dh_ore = p.dh * d.ore;  // TMP = DH*ORE*WWZ(K) (3dmhdsub.f:1363, 1380)
+    g->ph.id_dv_ore = p.dv * d.ore;
     g->ph.heat_on = p.itcon == 2 ? 1 : 0;
     g->ph.hh = p.hh;
     g->ph.hh_one = p.hh == 1.0 ? 1 : 0;
@@ -1179,6 +1213,7 @@ int r3d_gpu_fluxes(r3d_gpu* g, double* const* out) {
         if (!g || !out) throw std::invalid_argument("null argument");
         if (!g->uploaded) throw Error(R3D_ESTATE, "fluxes before upload");
         if (g->fp32) throw Error(R3D_EINVAL, "r3d_gpu_fluxes needs precision fp64");
+        if (g->p.id != 0) throw Error(R3D_EINVAL, "r3d_gpu_fluxes does not form the density diffusion (ID)");
         DeviceGuard dg(g->device);
         const Derived& d = g->d;
         const size_t fe = (size_t)g->geo.plane * d.nz;

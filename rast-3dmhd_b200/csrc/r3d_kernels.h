@@ -63,6 +63,10 @@ size_t stage_fp64_smem();
 int stage_fp64_rows(int mhd, int npx, int npy, int nloc, int num_sms);
 // resident CTAs per SM of the FP64 stage kernels (hydro: all three stages; MHD: by tile rows)
 int stage_fp64_ctas_per_sm(int mhd, int rows);
+// Horizontal means of rho per local plane (density diffusion): rom[k], and wwz[k] = 1/rom[k]
+// when id_mode == 1; the domain's ghost planes take the means of their mirror planes.
+cudaError_t launch_plane_mean(const Geometry& g, const double* ro, double* rom, double* wwz, int id_mode,
+                              cudaStream_t st);
 void stage_fp64_box(int rows, unsigned* bx, unsigned* by);
 cudaError_t launch_stage_fp64(int stage, const StageMaps& maps, const Geometry& g,
                               const Physics& ph, const Lines& L, const FieldSet& fs, Scalars* sc,

@@ -151,8 +151,9 @@ void stage_fp64_box(int rows, unsigned* bx, unsigned* by) {
     *by = rows + 2;
 }
 
-// TF (hydro, itcon 3 only): the top plane's flux is formed as on an interior plane (EdgeTag)
-template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV, bool TF = false>
+// TF (hydro, itcon 3 only): the top plane's flux is formed as on an interior plane (EdgeTag);
+// IDD (hydro, ID 1 or 2 only): the density diffusion is added to FR (itcon 3 then at run time)
+template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV, bool TF = false, bool IDD = false>
 __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, TYV>::min_blocks)
     stage_fp64(const __grid_constant__ StageMaps maps, Geometry g, Physics ph, Lines L,
                FieldSet fs, Scalars* sc, int kchunk) {
@@ -379,6 +380,27 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
             else
                 dwz = (RW_(rp, R_RW, 0, 0) - RM_(R_RW)) * tmpz;
             fr -= dwz;
+            if constexpr (IDD && !MHD) {
+                // ---- density diffusion (ID 1, 2), 3dmhdsub.f:1316-1386: WW1 = RO - ROM(K) ----
+                const double rmk = L.rom[k];
+                const double w0 = RW_(r0, R_RO, 0, 0) - rmk;
+                if (ph.id_dh != 0.0) {
+                    const double wxp = RW_(r0, R_RO, 1, 0) - rmk, wxm = RW_(r0, R_RO, -1, 0) - rmk;
+                    const double wyp = RW_(r0, R_RO, 0, 1) - rmk, wym = RW_(r0, R_RO, 0, -1) - rmk;
+                    const double ww2 = (wxp - wxm) * hx * d2x + d2sum(wxp, w0, wxm) * h2x * dx1 * dx1;  // :1349
+                    const double ww3 = (wyp - wym) * tmpy1 + d2sum(wyp, w0, wym) * tmpy2;                // :1358
+                    fr = fr + (ww2 + ww3) * (ph.id_dh_ore * L.wwz[k]);                                   // :1366
+                }
+                if (ph.id_dv != 0.0) {
+                    // rho at k-1, k+1; the domain's ghost planes hold their mirror planes (:1318, :1321)
+                    const double ro_m = fs.xin[R_RO][nc - PL], ro_p = RW_(rp, R_RO, 0, 0);
+                    const double rzp = (k == g.npz && g.bot_edge) ? ro_m : ro_p;
+                    const double rzm = (k == 1 && g.top_edge) ? ro_p : ro_m;
+                    const double wzp = rzp - L.rom[k + 1], wzm = rzm - L.rom[k - 1];
+                    const double ww2z = (wzp - wzm) * L.tmpz1[k] + d2sum(wzp, w0, wzm) * L.tmpz2[k];     // :1375
+                    fr = fr + ww2z * (ph.id_dv_ore * L.wwz[k]);                                          // :1383
+                }
+            }
 
             double fu = 0.0, fv = 0.0, fw = 0.0, ft = 0.0;
             double b1 = 0.0, b2f = 0.0, b3 = 0.0;  // B fluxes WW1..WW3 (MHD)
@@ -625,8 +647,8 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
         if (!edge) {
             rhs(EdgeTag<false>{});
         } else {
-            if constexpr (TF && !MHD) {
-                if (k == 1 && g.top_edge) rhs(EdgeTag<true, true>{});
+            if constexpr ((TF || IDD) && !MHD) {
+                if (k == 1 && g.top_edge && (TF || ph.top_free)) rhs(EdgeTag<true, true>{});
                 else rhs(EdgeTag<true>{});
             } else {
                 rhs(EdgeTag<true>{});
@@ -729,40 +751,44 @@ __global__ void __launch_bounds__(Cells<MHD, STAGE, TYV>::nt, Cells<MHD, STAGE, 
     if (STAGE == 2) reduce_dt(der, m1, m2, m3, m4, mu, sc);
 }
 
-template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV, bool TF>
+template <int STAGE, bool KC, bool MHD, bool EMIT, int TYV, bool TF, bool IDD>
 static void launch_one(dim3 grid, const StageMaps& maps, const Geometry& g, const Physics& ph,
                        const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
     static bool configured = false;
     constexpr size_t smem = Shape<MHD, TYV>::smem;
     if (!configured) {
-        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF, IDD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         // all of the unified L1 as shared memory, so that the resident CTAs fit
-        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF>,
+        cudaFuncSetAttribute(stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF, IDD>,
                              cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         configured = true;
     }
     const dim3 block(TX, TYV / Cells<MHD, STAGE, TYV>::cpt, 1);
-    stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
+    stage_fp64<STAGE, KC, MHD, EMIT, TYV, TF, IDD><<<grid, block, smem, st>>>(maps, g, ph, L, fs, sc, kchunk);
 }
 
-template <bool MHD, bool EMIT, int TYV, bool TF = false>
+template <bool MHD, bool EMIT, int TYV, bool TF = false, bool IDD = false>
 static void launch_stage(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                          const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
     const dim3 grid((g.npx + TX - 1) / TX, (g.npy + TYV - 1) / TYV, (g.npz + kchunk - 1) / kchunk);
     const bool kc = ph.kappa_const != 0;
-    if (stage == 0) kc ? launch_one<0, true, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st)
-                       : launch_one<0, false, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st);
-    else if (stage == 1) kc ? launch_one<1, true, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st)
-                            : launch_one<1, false, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st);
-    else kc ? launch_one<2, true, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st)
-            : launch_one<2, false, MHD, EMIT, TYV, TF>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+    if (stage == 0) kc ? launch_one<0, true, MHD, EMIT, TYV, TF, IDD>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+                       : launch_one<0, false, MHD, EMIT, TYV, TF, IDD>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+    else if (stage == 1) kc ? launch_one<1, true, MHD, EMIT, TYV, TF, IDD>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+                            : launch_one<1, false, MHD, EMIT, TYV, TF, IDD>(grid, maps, g, ph, L, fs, sc, kchunk, st);
+    else kc ? launch_one<2, true, MHD, EMIT, TYV, TF, IDD>(grid, maps, g, ph, L, fs, sc, kchunk, st)
+            : launch_one<2, false, MHD, EMIT, TYV, TF, IDD>(grid, maps, g, ph, L, fs, sc, kchunk, st);
 }
 
 template <bool EMIT>
 static void launch_any(int stage, const StageMaps& maps, const Geometry& g, const Physics& ph,
                        const Lines& L, const FieldSet& fs, Scalars* sc, int kchunk, cudaStream_t st) {
-    if constexpr (!EMIT) {  // itcon 3 (hydro; the adjoint's EMIT recompute refuses it)
+    if constexpr (!EMIT) {  // ID, itcon 3 (hydro; the adjoint's EMIT recompute refuses them)
+        if (!ph.lmag && ph.id_mode) {
+            launch_stage<false, false, R3D_STAGE_TY, false, true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
+            return;
+        }
         if (!ph.lmag && ph.top_free) {
             launch_stage<false, false, R3D_STAGE_TY, true>(stage, maps, g, ph, L, fs, sc, kchunk, st);
             return;

@@ -108,7 +108,14 @@ void check_params(const r3d_params& p) {
     if (p.lshr) bad("LSHR is not supported (the reference aborts too)");
     if (p.lrem) bad("LREM is not supported (the reference aborts too)");
     if (p.rlax > 0.0) bad("flux relaxation (RLAX) is not supported (the reference aborts too)");
-    if (p.id != 0) bad("density diffusion ID is not supported (the reference aborts too)");
+    if (p.id != 0) {
+        // density diffusion, 3dmhdsub.f:1316-1386: its HORIZONTAL_MEAN exists for the uniform
+        // grid only (3dmhdsub.f:3187-3190 stops otherwise)
+        if (p.id != 1 && p.id != 2) bad("ID must be 0, 1 or 2");
+        if (p.ngrid != 0) bad("ID (density diffusion) needs the uniform grid --ngrid 0, as the Fortran does");
+        if (p.precision != R3D_PREC_FP64 || p.lmag)
+            bad("ID (density diffusion) is available in the fp64 hydro form only");
+    }
     if (!(p.itcon >= 0 && p.itcon <= 4)) bad("ITCON must be 0 .. 4 (others leave the top plane undefined)");
     if (p.itcon == 2 && p.precision != R3D_PREC_FP64)
         bad("ITCON 2 (embedded heat loss) is available in the fp64 form only");

@@ -42,6 +42,15 @@ HYDRO_CASES = [
     ("itcon3_variable_kappa_izcon1", ["--npx", "21", "--npy", "17", "--npz", "30", "--itcon", "3",
                                       "--izcon", "1", "--ngrid", "2", "--pzp", "0.5", "--sigma", "0.1",
                                       "--polys", "1.5"], 7, 5),
+    # density diffusion (ID 1, 2; 3dmhdsub.f:1316-1386, uniform grid; the oracle's term is pinned
+    # to that source, test_oracle_id_pin.py): horizontal, vertical, both with the ID 2 profile,
+    # and with a free top temperature on a ragged grid
+    ("id1_dh", ["--npx", "24", "--npy", "20", "--npz", "36", "--ngrid", "0", "--id", "1", "--dh", "0.5"], 5, 4),
+    ("id1_dv", ["--npx", "24", "--npy", "20", "--npz", "36", "--ngrid", "0", "--id", "1", "--dv", "0.75"], 5, 4),
+    ("id2_dh_dv", ["--npx", "24", "--npy", "20", "--npz", "36", "--ngrid", "0", "--id", "2", "--dh", "0.25",
+                   "--dv", "0.25", "--zmax", "2"], 7, 4),
+    ("id1_itcon3_ragged", ["--npx", "21", "--npy", "17", "--npz", "30", "--ngrid", "0", "--id", "1", "--dh", "0.5",
+                           "--dv", "0.5", "--itcon", "3", "--tp", "0.5"], 3, 5),
 ]
 
 

@@ -19,6 +19,8 @@ CASES = [
     ("variable_kappa", ["--npx", "24", "--npy", "20", "--npz", "30", "--pzp", "0.5", "--sigma", "0.1",
                         "--polys", "1.5"], (3,)),
     ("itcon3", ["--npx", "24", "--npy", "16", "--npz", "30", "--itcon", "3", "--tp", "0.5"], (2, 3)),
+    ("id1_dh_dv", ["--npx", "24", "--npy", "16", "--npz", "30", "--ngrid", "0", "--id", "1", "--dh", "0.5",
+                   "--dv", "0.5"], (2, 3)),
     ("mhd", ["--npx", "24", "--npy", "20", "--npz", "40"] + MAG, (2, 3)),
     ("fp32bulk", ["--npx", "40", "--npy", "24", "--npz", "32", "--precision", "fp32bulk"], (2, 4)),
 ]

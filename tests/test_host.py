@@ -77,7 +77,10 @@ def test_parser_rejects_unknown_and_missing_values():
     (["--ix", "4"], "stencil"), (["--lrem", "1"], "LREM"), (["--lshr", "1"], "LSHR"),
     (["--rlax", "0.5"], "RLAX"), (["--id", "1"], "ID"), (["--itcon", "2", "--precision", "fp32bulk"], "ITCON 2"),
     (["--itcon", "3", "--precision", "fp32bulk"], "ITCON 3"), (["--itcon", "3", "--lmag", "1"], "ITCON 3"),
-    (["--itcon", "5"], "ITCON"), (["--izcon", "2"], "IZCON"), (["--ixcon", "1"], "periodic"),
+    (["--itcon", "5"], "ITCON"), (["--izcon", "2"], "IZCON"),
+    (["--id", "1", "--ngrid", "2"], "uniform grid"), (["--id", "3", "--ngrid", "0"], "ID must be"),
+    (["--id", "1", "--ngrid", "0", "--precision", "fp32bulk"], "ID (density"),
+    (["--id", "2", "--ngrid", "0", "--lmag", "1", "--beta", "10", "--rm", "1"], "ID (density"), (["--ixcon", "1"], "periodic"),
     (["--nstart", "3"], "restart"), (["--ampb", "0.1"], "AMPB"),
     (["--lmag", "1", "--rm", "0", "--beta", "1"], "LMAG"), (["--seed", "0"], "seed"),
     (["--npz", "4"], "too small"),
