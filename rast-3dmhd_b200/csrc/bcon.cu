@@ -105,32 +105,54 @@ __global__ void __launch_bounds__(256) bcon_kernel(Geometry g, Physics ph, Lines
 // Horizontal mean of rho per plane for the density diffusion (ID 1, 2): HORIZONTAL_MEAN of the
 // Fortran (3dmhdsub.f:3177-3186, the uniform grid it requires, one rank in y): the plane's
 // interior values added in loop order (j outer, i inner) and divided by FLOAT(NPX*NPY).  One
-// thread per plane keeps that order exactly.  The domain's ghost planes are first loaded with
-// their mirror planes (3dmhdsub.f:1318, 1321), so their means are those of planes 2 and npz-1.
+// CTA per plane: its other warps stage the plane in chunks of kMeanChunk values (in that
+// order, coalesced, double-buffered in shared memory) while thread 0 adds them one by one, so
+// the order is exactly the Fortran's.  The domain's ghost planes are first loaded with their
+// mirror planes (3dmhdsub.f:1318, 1321), so their means are those of planes 2 and npz-1.
 // ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) plane_mean_kernel(Geometry g, const double* ro, double* rom, double* wwz,
-                                                          int id_mode) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k > g.npz + 1) return;
+constexpr int kMeanChunk = 2048, kMeanThreads = 256;
+
+__global__ void __launch_bounds__(kMeanThreads) plane_mean_kernel(Geometry g, const double* ro, double* rom,
+                                                                   double* wwz, int id_mode) {
+    __shared__ double buf[2][kMeanChunk];
+    const int k = blockIdx.x;  // local plane 0 .. npz+1
     int src = k;
     if (k == 0 && g.top_edge) src = 2;
     if (k == g.npz + 1 && g.bot_edge) src = g.npz - 1;
     const double* p = ro + (int64_t)src * g.plane;
+    const int64_t nval = (int64_t)g.npx * g.npy;
+    const int nchunk = (int)((nval + kMeanChunk - 1) / kMeanChunk);
+    // value t of the plane in (j, i) order: row 1 + t / npx, column 1 + t % npx
+    auto load = [&](int c, double* b) {
+        if (threadIdx.x < 32) return;  // warp 0 adds
+        const int64_t t0 = (int64_t)c * kMeanChunk;
+        for (int u = threadIdx.x - 32; u < kMeanChunk; u += kMeanThreads - 32) {
+            const int64_t t = t0 + u;
+            if (t < nval) b[u] = p[(1 + t / g.npx) * g.pitch + 1 + t % g.npx];
+        }
+    };
+    load(0, buf[0]);
+    __syncthreads();
     double sum = 0.0;
-    for (int j = 1; j <= g.npy; ++j) {
-        const double* r = p + (int64_t)j * g.pitch;
-#pragma unroll 8
-        for (int i = 1; i <= g.npx; ++i) sum = sum + r[i];
+    for (int c = 0; c < nchunk; ++c) {
+        if (c + 1 < nchunk) load(c + 1, buf[(c + 1) & 1]);
+        if (threadIdx.x == 0) {
+            const double* b = buf[c & 1];
+            const int n = (int)min((int64_t)kMeanChunk, nval - (int64_t)c * kMeanChunk);
+            for (int u = 0; u < n; ++u) sum = sum + b[u];
+        }
+        __syncthreads();
     }
-    const double m = sum / (double)(float)(g.npx * g.npy);
-    rom[k] = m;
-    if (id_mode == 1) wwz[k] = 1.0 / m;  // WWZ = 1.0E00/ROM (3dmhdsub.f:1338)
+    if (threadIdx.x == 0) {
+        const double m = sum / (double)(float)(g.npx * g.npy);
+        rom[k] = m;
+        if (id_mode == 1) wwz[k] = 1.0 / m;  // WWZ = 1.0E00/ROM (3dmhdsub.f:1338)
+    }
 }
 
 cudaError_t launch_plane_mean(const Geometry& g, const double* ro, double* rom, double* wwz, int id_mode,
                               cudaStream_t st) {
-    const int n = g.npz + 2;
-    plane_mean_kernel<<<(n + 127) / 128, 128, 0, st>>>(g, ro, rom, wwz, id_mode);
+    plane_mean_kernel<<<g.npz + 2, kMeanThreads, 0, st>>>(g, ro, rom, wwz, id_mode);
     return cudaGetLastError();
 }
 
