@@ -162,7 +162,8 @@ int r3d_mesh_debug_dt_filter(r3d_mesh* m, double margin, int* refolds);
  * FU FV FW FR FT (+ the B fluxes WW1 WW2 WW3), interior cells, ghosts 0.  On the domain's top
  * and bottom planes the momentum and energy right-hand sides, which BCON overwrites, are
  * returned as 0; the continuity and B fluxes there are the reference's one-sided forms.
- * FP64 only. */
+ * FP64 only; refused (R3D_EINVAL) with the density diffusion (ID), which exists only inside a
+ * stage, after its per-plane means. */
 int r3d_gpu_fluxes(r3d_gpu* g, double* const* out);
 
 /* Test hook for the failure path: from the next step on, every TMA transaction of the stage
