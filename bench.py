@@ -257,6 +257,51 @@ def cpu_reference_sample(warmup: int = 1, nsteps: int = 2):
                           f"{nsteps} timed steps ({e})"}
 
 
+REF_GPU_RANKS = 2  # the reference needs NPEZ >= 2 (src/topology.cpp:50-55)
+
+
+def reference_gpu_leg(warmup: int = 1, nsteps: int = 3):
+    """The reference's own GPU driver (src/gpu.cpp + src/gpu_kernels.cu, unmodified, sm_100a, its
+    stock host-staged build) on the benchmark grid: the reference set-up, then `warmup` untimed
+    and `nsteps` timed step_gpu calls on two thread-ranks in z sharing this GPU, the device
+    synchronised and the ranks joined on both sides (host clock: the driver's own stream is not
+    reachable from here)."""
+    from oracle import Reference
+
+    cells = GRID[0] * GRID[1] * GRID[2]
+    sc, sec = Reference.time_gpu(FLAGS + ["--npey", "1"], REF_GPU_RANKS, SEED, warmup, nsteps)
+    return {"value": cells * nsteps / sec / 1e6, "unit": UNIT, "ms_per_step": sec / nsteps * 1e3,
+            "steps": nsteps, "warmup": warmup, "final_dt": sc["dt"], "ranks": REF_GPU_RANKS}
+
+
+def reference_gpu_run(fp64_ms_per_step, limit_s: float = 600.0):
+    """reference_gpu_leg in a child process (the driver exits its process on a CUDA error,
+    src/gpu.cpp:117-126), set beside the fused FP64 step."""
+    from oracle import Reference
+
+    if not Reference.gpu_available():
+        return {"unavailable": "reference GPU driver not built (the reference tree was absent at build time)"}
+    t0 = time.perf_counter()
+    try:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--reference-gpu-leg"],
+                           capture_output=True, text=True, timeout=limit_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"reference GPU leg did not finish within {limit_s:.0f} s"}
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr.strip().splitlines() or ["no output"])[-1]
+        return {"unavailable": f"reference GPU leg failed (rc {r.returncode}): {tail[:200]}"}
+    out = json.loads(lines[-1])
+    out["fused_fp64_speedup"] = out["ms_per_step"] / fp64_ms_per_step
+    out["wall_s"] = time.perf_counter() - t0
+    out["note"] = (f"the reference's stock GPU build (host-staged halos, host-side dt minimum: four "
+                   f"whole arrays copied to the host per step, src/gpu.cpp:787-823), its set-up and "
+                   f"grid {GRID[0]}x{GRID[1]}x{GRID[2]} seed {SEED}, {REF_GPU_RANKS} thread-ranks in z "
+                   f"on this GPU, host clock around synchronised steps; the NCCL build "
+                   f"(R3D_COMM_NCCL) needs one GPU per rank")
+    return out
+
+
 def side_run(R, flags, steps, warmup, bytes_per_cell, fp64_ms_per_step):
     """Timed run of another form of the step (same protocol as the headline, events on the
     library stream); returns Mcell-updates/s, % of the HBM roofline by its own algorithmic bytes
@@ -485,6 +530,8 @@ def main():
                     help="start and join the ranks (gloo) and report them, without GPU work")
     ap.add_argument("--adjoint", type=int, nargs=2, metavar=("STEPS", "EVERY"),
                     help="only the adjoint leg (MHD 64x64x128), STEPS recorded with a checkpoint every EVERY")
+    ap.add_argument("--reference-gpu-leg", action="store_true",
+                    help="only the reference's own GPU driver on the benchmark grid (or --grid), printed as one line")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return spawn_ranks(args.gpus)
@@ -503,6 +550,9 @@ def main():
     if args.grid:
         GRID = tuple(args.grid)
         FLAGS = ["--npx", str(GRID[0]), "--npy", str(GRID[1]), "--npz", str(GRID[2])]
+    if args.reference_gpu_leg:
+        emit(reference_gpu_leg())
+        return 0
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local, pg = dist_init()
@@ -623,6 +673,7 @@ def main():
         extra["fp32bulk_error_504x504x512_100steps"] = fp32_error_run(R, local, GRID, 100)
         extra["fp32bulk_plume_504x504x2048_50steps"] = fp32_error_run(R, local, (504, 504, 2048), 50,
                                                                               PLUME, seed=11)
+        extra["reference_gpu_driver_504x504x512"] = reference_gpu_run(ms_per_step)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         cpu = cpu_reference_sample()

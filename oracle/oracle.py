@@ -2,7 +2,9 @@
 
 * ``Oracle``    - the C restatement in r3d_oracle.c (always available once built).
 * ``Reference`` - the reference's own CPU sources compiled unmodified into
-  _ref/libr3dref.so (present where the reference tree was available at build time).
+  _ref/libr3dref.so (present where the reference tree was available at build time); with
+  ``run_gpu`` / ``time_gpu`` the same set-up followed by the reference's own GPU driver
+  (src/gpu.cpp, src/gpu_kernels.cu for sm_100a, one copy per thread-rank, _ref/libr3dgpu_r*.so).
 
 Both take reference-style CLI flags (src/params.cpp:113-224) and return global
 (npx+2) x (npy+2) x (npz+2) arrays shaped (NZ, NY, NX).  Only tests/, the smoke check and
@@ -19,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libr3dref.so")
+REF_GPU_COPIES = [os.path.join(HERE, "_ref", f"libr3dgpu_r{r}.so") for r in range(8)]
 
 FIELDS = ["ru", "rv", "rw", "ro", "tt", "uu", "vv", "ww", "fu", "fv", "fw", "fr", "ft",
           "zru", "zrv", "zrw", "zro", "ztt", "ww1", "ww2", "ww3", "bx", "by", "bz",
@@ -180,6 +183,10 @@ class Reference:
         return os.path.exists(REF_SO)
 
     @classmethod
+    def gpu_available(cls) -> bool:
+        return cls.available() and all(os.path.exists(c) for c in REF_GPU_COPIES)
+
+    @classmethod
     def lib(cls):
         if cls._lib is None:
             if not os.path.exists(REF_SO):
@@ -192,6 +199,10 @@ class Reference:
             lib.ref_ran2.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
             lib.ref_time.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+            lib.ref_run_gpu.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+            lib.ref_time_gpu.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
             cls._lib = lib
         return cls._lib
 
@@ -235,6 +246,34 @@ class Reference:
         arr, n = _argv(args)
         rc = cls.lib().ref_time(arr, n, nranks, seed, warmup, nsteps, omp_threads, sc.ctypes.data,
                                 secs.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(cls.lib().ref_last_error().decode())
+        return dict(zip(SCALARS, sc.tolist())), float(secs[0])
+
+    @classmethod
+    def run_gpu(cls, args: Sequence[str], nranks: int = 2, seed: int = 62659, nsteps: int = 0,
+                last_stages: int = 3):
+        """Set-up + nsteps steps of the reference GPU driver (needs a GPU: the driver exits the
+        process on a CUDA error, src/gpu.cpp:117-126); returns (fields, scalars, seconds)."""
+        npx, npy, npz = grid_of(args)
+        out3 = np.zeros((8, npz + 2, npy + 2, npx + 2))
+        sc = np.zeros(7)
+        secs = np.zeros(1)
+        arr, n = _argv(args)
+        rc = cls.lib().ref_run_gpu(arr, n, nranks, seed, nsteps, last_stages, out3.ctypes.data,
+                                   sc.ctypes.data, secs.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(cls.lib().ref_last_error().decode())
+        return dict(zip(PRIMARY, out3)), dict(zip(SCALARS, sc.tolist())), float(secs[0])
+
+    @classmethod
+    def time_gpu(cls, args: Sequence[str], nranks: int, seed: int, warmup: int, nsteps: int):
+        """Set-up, `warmup` untimed and `nsteps` timed steps of the reference GPU driver, the
+        device synchronised and the ranks joined on both sides; returns (scalars, seconds)."""
+        sc = np.zeros(7)
+        secs = np.zeros(1)
+        arr, n = _argv(args)
+        rc = cls.lib().ref_time_gpu(arr, n, nranks, seed, warmup, nsteps, sc.ctypes.data, secs.ctypes.data)
         if rc != 0:
             raise RuntimeError(cls.lib().ref_last_error().decode())
         return dict(zip(SCALARS, sc.tolist())), float(secs[0])

@@ -13,6 +13,12 @@
 // z-rank, local k, y-rank, then the nry x npx plane x-fastest; each plane value is
 // 1 + ampt*(ran2()-0.5) and multiplies TT.  Seed 62659 through this path equals the stock path
 // bit for bit (checked by tests/test_oracle_ref.py).
+//
+// GPU mode (ref_run_gpu, ref_time_gpu): after the same set-up, every thread-rank runs the
+// reference's own GPU time loop (src/main.cpp:234-275: gpu_alloc, gpu_upload, step_gpu,
+// gpu_download) through its own copy of the reference GPU driver, _ref/libr3dgpu_r<rank>.so
+// (see ref_gpu_entry.cpp); all ranks share the one device.
+#include <dlfcn.h>
 #include <omp.h>
 
 #include <algorithm>
@@ -21,6 +27,8 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <mutex>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -47,6 +55,7 @@ struct Job {
     int omp_threads = 1;
     int fluxes_only = 0;  // after nsteps, run one FLUXES and return FU..FT in place of state
     int warmup = 0;       // untimed steps before the timed nsteps (timing runs)
+    int gpu = 0;          // step with the reference GPU driver instead of src/step.cpp
     // outputs (global arrays, may be null)
     double* out3d = nullptr;   // 8 x NX*NY*NZ : ru rv rw ro tt bx by bz (or fu fv fw fr ft ...)
     double* out1d = nullptr;   // 14 x (NX | NY | NZ) packed: exx.. (NX) wyy.. (NY) zee.. (NZ) rkapa dkapa (NZ)
@@ -131,6 +140,49 @@ void gather1d(const r3d::Params& p, const r3d::Derived& d, const r3d::Topology& 
         }
 }
 
+// One copy of the reference GPU driver (ref_gpu_entry.cpp), opened once per rank index and kept
+// for the life of the process.
+struct GpuCopy {
+    void* (*alloc)(const r3d::Derived*) = nullptr;
+    void (*upload)(void*, const r3d::SimState*) = nullptr;
+    void (*download)(r3d::SimState*, void*) = nullptr;
+    void (*step)(int, const r3d::Params*, const r3d::Derived*, const r3d::Topology*, void*, r3d::SimState*) = nullptr;
+    void (*free_)(void*) = nullptr;
+    int (*sync)(void) = nullptr;
+};
+
+constexpr int kMaxGpuCopies = 8;  // the copies oracle/Makefile builds
+
+const GpuCopy& gpu_copy(int rank) {
+    static std::mutex mu;
+    static GpuCopy copies[kMaxGpuCopies];
+    if (rank < 0 || rank >= kMaxGpuCopies) throw std::runtime_error("ref gpu: more ranks than driver copies");
+    std::lock_guard<std::mutex> lk(mu);
+    GpuCopy& c = copies[rank];
+    if (c.alloc) return c;
+    Dl_info info;
+    if (!dladdr((void*)&gpu_copy, &info) || !info.dli_fname) throw std::runtime_error("ref gpu: dladdr failed");
+    std::string dir(info.dli_fname);
+    dir = dir.substr(0, dir.rfind('/') + 1);
+    const std::string path = dir + "libr3dgpu_r" + std::to_string(rank) + ".so";
+    void* h = dlopen(path.c_str(), RTLD_NOW | RTLD_LOCAL);
+    if (!h) throw std::runtime_error(std::string("ref gpu: ") + dlerror());
+    auto sym = [&](const char* name) {
+        void* f = dlsym(h, name);
+        if (!f) throw std::runtime_error(std::string("ref gpu: missing ") + name + " in " + path);
+        return f;
+    };
+    GpuCopy n;
+    n.alloc = (decltype(n.alloc))sym("r3dg_alloc");
+    n.upload = (decltype(n.upload))sym("r3dg_upload");
+    n.download = (decltype(n.download))sym("r3dg_download");
+    n.step = (decltype(n.step))sym("r3dg_step");
+    n.free_ = (decltype(n.free_))sym("r3dg_free");
+    n.sync = (decltype(n.sync))sym("r3dg_sync");
+    c = n;
+    return c;
+}
+
 void rank_main(Job& job, int rank) {
     r3d_shim_bind_rank(rank);
     omp_set_num_threads(job.omp_threads);
@@ -171,17 +223,37 @@ void rank_main(Job& job, int rank) {
     s.timi = 0.0;
     r3d::communicate(MPI_COMM_WORLD, p, t, s);
 
-    for (int n = 1; n <= job.warmup; ++n) r3d::step(3, MPI_COMM_WORLD, p, d, t, s);
     double wbuf[1] = {0.0}, wout[1];
-    MPI_Allreduce(wbuf, wout, 1, MPI_DOUBLE, MPI_MIN, MPI_COMM_WORLD);
-    auto t0 = std::chrono::steady_clock::now();
-    for (int n = 1; n <= job.nsteps; ++n) {
-        int ns = (n == job.nsteps) ? job.last_stages : 3;
-        r3d::step(ns, MPI_COMM_WORLD, p, d, t, s);
+    if (job.gpu) {
+        // src/main.cpp:238-275; the rank's SimState is its own scalar mirror (step_gpu touches
+        // only dt, nit, timc, timt, timi and tb of it)
+        const GpuCopy& c = gpu_copy(rank);
+        void* g = c.alloc(&d);
+        c.upload(g, &s);
+        for (int n = 1; n <= job.warmup; ++n) c.step(3, &p, &d, &t, g, &s);
+        if (c.sync() != 0) throw std::runtime_error("ref gpu: device error before the timed steps");
+        MPI_Allreduce(wbuf, wout, 1, MPI_DOUBLE, MPI_MIN, MPI_COMM_WORLD);
+        auto t0 = std::chrono::steady_clock::now();
+        for (int n = 1; n <= job.nsteps; ++n) c.step((n == job.nsteps) ? job.last_stages : 3, &p, &d, &t, g, &s);
+        const int rc = c.sync();
+        MPI_Allreduce(wbuf, wout, 1, MPI_DOUBLE, MPI_MIN, MPI_COMM_WORLD);
+        auto t1 = std::chrono::steady_clock::now();
+        if (rc != 0) throw std::runtime_error("ref gpu: device error in the timed steps");
+        if (rank == 0 && job.seconds) *job.seconds = std::chrono::duration<double>(t1 - t0).count();
+        if (job.out3d) c.download(&s, g);
+        c.free_(g);
+    } else {
+        for (int n = 1; n <= job.warmup; ++n) r3d::step(3, MPI_COMM_WORLD, p, d, t, s);
+        MPI_Allreduce(wbuf, wout, 1, MPI_DOUBLE, MPI_MIN, MPI_COMM_WORLD);
+        auto t0 = std::chrono::steady_clock::now();
+        for (int n = 1; n <= job.nsteps; ++n) {
+            int ns = (n == job.nsteps) ? job.last_stages : 3;
+            r3d::step(ns, MPI_COMM_WORLD, p, d, t, s);
+        }
+        MPI_Allreduce(wbuf, wout, 1, MPI_DOUBLE, MPI_MIN, MPI_COMM_WORLD);
+        auto t1 = std::chrono::steady_clock::now();
+        if (rank == 0 && job.seconds) *job.seconds = std::chrono::duration<double>(t1 - t0).count();
     }
-    MPI_Allreduce(wbuf, wout, 1, MPI_DOUBLE, MPI_MIN, MPI_COMM_WORLD);
-    auto t1 = std::chrono::steady_clock::now();
-    if (rank == 0 && job.seconds) *job.seconds = std::chrono::duration<double>(t1 - t0).count();
 
     if (job.fluxes_only) {
         r3d::fluxes(p, d, t, s.rkapa.data(), s.dkapa.data(), s);
@@ -265,6 +337,37 @@ int ref_time(const char** args, int nargs, int nranks, int seed, int warmup, int
     job.warmup = warmup;
     job.nsteps = nsteps;
     job.omp_threads = omp_threads;
+    job.scalars = scalars;
+    job.seconds = seconds;
+    return run_job(job);
+}
+
+// The same two runs with the reference's own GPU driver (src/gpu.cpp) on every thread-rank:
+// state after nsteps (ru rv rw ro tt bx by bz, downloaded as src/main.cpp:273 does) and timing.
+int ref_run_gpu(const char** args, int nargs, int nranks, int seed, int nsteps, int last_stages,
+                double* out3d, double* scalars, double* seconds) {
+    Job job;
+    for (int i = 0; i < nargs; ++i) job.args.emplace_back(args[i]);
+    job.nranks = nranks;
+    job.seed = seed;
+    job.nsteps = nsteps;
+    job.last_stages = last_stages;
+    job.gpu = 1;
+    job.out3d = out3d;
+    job.scalars = scalars;
+    job.seconds = seconds;
+    return run_job(job);
+}
+
+int ref_time_gpu(const char** args, int nargs, int nranks, int seed, int warmup, int nsteps, double* scalars,
+                 double* seconds) {
+    Job job;
+    for (int i = 0; i < nargs; ++i) job.args.emplace_back(args[i]);
+    job.nranks = nranks;
+    job.seed = seed;
+    job.warmup = warmup;
+    job.nsteps = nsteps;
+    job.gpu = 1;
     job.scalars = scalars;
     job.seconds = seconds;
     return run_job(job);

@@ -1,0 +1,103 @@
+"""The reference's own GPU driver: src/gpu.cpp and src/gpu_kernels.cu compiled unmodified for
+sm_100a (oracle/Makefile), one copy per thread-rank, run behind the reference's set-up by the
+oracle harness.  It is the comparison build for the B200 path's throughput, so it must compute
+what the reference computes.
+
+CPU: the copies exist as separate files (each rank needs its own function-level statics,
+src/gpu.cpp:406-459) and export their entry points.  GPU, on the B200:
+
+* without the plume forcing (--tp 0), over the three steps the reference's gpu_equivalence_test
+  runs (tests/gpu_equivalence_test.cpp:25, 120-175), on two ranks in z and on four ranks two in
+  y, the driver reproduces the reference CPU build bit for bit: every primary field, dt, TIMC,
+  NIT;
+* over longer runs its dt departs first: the GPU step takes the advective limit from a stale UU
+  (k_step_uu is never launched; the limits come from WW1..WW3 of k_step_dt, src/gpu.cpp:787-823),
+  so from some step on its dt differs from the CPU build's, and the state follows;
+* with the plume (the default, tp = 2) its BCON forms the two Gaussian factors differently from
+  the CPU build: exponent cln*((x-xp)*(x-xp)) and the device exp (src/gpu_kernels.cu:739-741)
+  against (cln*(x-xp))*(x-xp) and the host libm exp (src/bcon.cpp:52-55), which differ in the
+  last bit for some cells.  (The B200 library builds those factors on the host in the CPU
+  build's form and stays bit-exact with it, tests/test_gpu_parity.py.)
+
+UMACH is not compared: the reference GPU step never forms it (src/gpu.cpp:736-1047).
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import REF_GPU_COPIES, PRIMARY, Reference, interior
+
+pytestmark = pytest.mark.skipif(not Reference.gpu_available(), reason="reference GPU driver not built")
+
+ENTRY = ["r3dg_alloc", "r3dg_upload", "r3dg_download", "r3dg_step", "r3dg_free", "r3dg_sync"]
+
+
+def test_driver_copies_are_separate_and_export_entry_points():
+    inodes = {os.stat(c).st_ino for c in REF_GPU_COPIES}
+    assert len(inodes) == len(REF_GPU_COPIES)
+    Reference.lib()  # the copies take MPI from the loaded stand-in
+    for c in REF_GPU_COPIES[:2]:
+        lib = ctypes.CDLL(c, mode=os.RTLD_LOCAL)
+        for name in ENTRY:
+            assert hasattr(lib, name), (c, name)
+
+
+CASES = [
+    # (flags, nranks, seed, steps)
+    (["--npx", "32", "--npy", "32", "--npz", "64", "--npey", "1", "--tp", "0"], 2, 1, 3),
+    (["--npx", "16", "--npy", "16", "--npz", "32", "--npey", "2", "--tp", "0"], 4, 62659, 3),
+]
+
+
+def both(flags, nranks, seed, steps):
+    gf, gs, _ = Reference.run_gpu(flags, nranks=nranks, seed=seed, nsteps=steps)
+    cf, _, cs, _ = Reference.run(flags, nranks=nranks, seed=seed, nsteps=steps, omp_threads=2)
+    return gf, gs, cf, cs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flags,nranks,seed,steps", CASES)
+def test_reference_gpu_driver_equals_reference_cpu(flags, nranks, seed, steps):
+    gf, gs, cf, cs = both(flags, nranks, seed, steps)
+    for n in PRIMARY[:5]:
+        d = float(np.abs(interior(gf[n]) - interior(cf[n])).max())
+        assert d == 0.0, (n, d)
+    for k in ("dt", "timc", "nit"):
+        assert gs[k] == cs[k], k
+
+
+@pytest.mark.gpu
+def test_reference_gpu_driver_dt_departs_before_the_state():
+    """Config 1's grid without the plume, steps 1..20: the first step whose state differs from
+    the CPU build's is one whose dt already differs (the state is a function of the previous state
+    and dt, so equal inputs give an equal step)."""
+    flags = ["--npx", "32", "--npy", "32", "--npz", "64", "--npey", "1", "--tp", "0"]
+    first_dt = first_state = None
+    for n in range(1, 21):
+        gf, gs, cf, cs = both(flags, 2, 1, n)
+        if first_dt is None and gs["dt"] != cs["dt"]:
+            first_dt = n
+        same = all(np.array_equal(interior(gf[f]), interior(cf[f])) for f in PRIMARY[:5])
+        if first_state is None and not same:
+            first_state = n
+            break
+    assert first_state is not None, "the builds agree over 20 steps"
+    assert first_dt is not None and first_dt <= first_state, (first_dt, first_state)
+
+
+@pytest.mark.gpu
+def test_reference_gpu_driver_plume_differs_by_device_exp_only():
+    """Config 1 (default plume, 20 steps): the reference GPU driver stays within 1e-12 of its CPU
+    build relative to each field's largest value; at these parameters the diffusive limit sets dt,
+    so the gap is the plume factors'."""
+    gf, gs, cf, cs = both(["--npx", "32", "--npy", "32", "--npz", "64", "--npey", "1"], 2, 1, 20)
+    worst = 0.0
+    for n in PRIMARY[:5]:
+        a, b = interior(gf[n]), interior(cf[n])
+        scale = float(np.abs(b).max())
+        worst = max(worst, float(np.abs(a - b).max()) / scale)
+    assert 0.0 < worst < 1e-12, worst
+    assert abs(gs["dt"] - cs["dt"]) <= 1e-12 * cs["dt"]
+    assert gs["nit"] == cs["nit"]
