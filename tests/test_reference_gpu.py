@@ -10,9 +10,10 @@ src/gpu.cpp:406-459) and export their entry points.  GPU, on the B200:
   runs (tests/gpu_equivalence_test.cpp:25, 120-175), on two ranks in z and on four ranks two in
   y, the driver reproduces the reference CPU build bit for bit: every primary field, dt, TIMC,
   NIT;
-* over longer runs its dt departs first: the GPU step takes the advective limit from a stale UU
-  (k_step_uu is never launched; the limits come from WW1..WW3 of k_step_dt, src/gpu.cpp:787-823),
-  so from some step on its dt differs from the CPU build's, and the state follows;
+* over longer runs it departs at the last-bit level: on config 1's grid without the plume the
+  state first differs at step 19 with dt still equal, so some per-cell expression of the GPU
+  kernels rounds differently from the CPU sweeps on states reached only later (not the dt: its
+  stale UU, k_step_uu never being launched, src/gpu.cpp:787-823, does not set dt here);
 * with the plume (the default, tp = 2) its BCON forms the two Gaussian factors differently from
   the CPU build: exponent cln*((x-xp)*(x-xp)) and the device exp (src/gpu_kernels.cu:739-741)
   against (cln*(x-xp))*(x-xp) and the host libm exp (src/bcon.cpp:52-55), which differ in the
@@ -69,22 +70,22 @@ def test_reference_gpu_driver_equals_reference_cpu(flags, nranks, seed, steps):
 
 
 @pytest.mark.gpu
-def test_reference_gpu_driver_dt_departs_before_the_state():
-    """Config 1's grid without the plume, steps 1..20: the first step whose state differs from
-    the CPU build's is one whose dt already differs (the state is a function of the previous state
-    and dt, so equal inputs give an equal step)."""
+def test_reference_gpu_driver_departs_late_and_by_the_last_bits():
+    """Config 1's grid without the plume, steps 1..20: equal for well beyond the reference's own
+    three steps, the first difference comes with dt still equal, and after 20 steps every field
+    is within 1e-12 of the CPU build's relative to its largest value."""
     flags = ["--npx", "32", "--npy", "32", "--npz", "64", "--npey", "1", "--tp", "0"]
-    first_dt = first_state = None
+    first = None
     for n in range(1, 21):
         gf, gs, cf, cs = both(flags, 2, 1, n)
-        if first_dt is None and gs["dt"] != cs["dt"]:
-            first_dt = n
         same = all(np.array_equal(interior(gf[f]), interior(cf[f])) for f in PRIMARY[:5])
-        if first_state is None and not same:
-            first_state = n
-            break
-    assert first_state is not None, "the builds agree over 20 steps"
-    assert first_dt is not None and first_dt <= first_state, (first_dt, first_state)
+        if not same and first is None:
+            first = n
+            assert gs["dt"] == cs["dt"], n
+    assert first is not None and first > 3, first
+    worst = max(float(np.abs(interior(gf[f]) - interior(cf[f])).max()) / float(np.abs(interior(cf[f])).max())
+                for f in PRIMARY[:5])
+    assert worst < 1e-12, worst
 
 
 @pytest.mark.gpu
