@@ -11,9 +11,9 @@ src/gpu.cpp:406-459) and export their entry points.  GPU, on the B200:
   y, the driver reproduces the reference CPU build bit for bit: every primary field, dt, TIMC,
   NIT;
 * over longer runs it departs at the last-bit level: on config 1's grid without the plume the
-  state first differs at step 19 with dt still equal, so some per-cell expression of the GPU
-  kernels rounds differently from the CPU sweeps on states reached only later (not the dt: its
-  stale UU, k_step_uu never being launched, src/gpu.cpp:787-823, does not set dt here);
+  state first differs at step 19 with dt still equal, so the difference arises inside the step
+  (its source in the GPU kernels is not identified; it is not the dt, whose stale UU,
+  k_step_uu never being launched, src/gpu.cpp:787-823, does not set dt here);
 * with the plume (the default, tp = 2) its BCON forms the two Gaussian factors differently from
   the CPU build: exponent cln*((x-xp)*(x-xp)) and the device exp (src/gpu_kernels.cu:739-741)
   against (cln*(x-xp))*(x-xp) and the host libm exp (src/bcon.cpp:52-55), which differ in the
