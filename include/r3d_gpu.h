@@ -166,6 +166,16 @@ int r3d_mesh_debug_dt_filter(r3d_mesh* m, double margin, int* refolds);
  * stage, after its per-plane means. */
 int r3d_gpu_fluxes(r3d_gpu* g, double* const* out);
 
+/* The FLUXES work arrays of the reference's gstate dump (src/main.cpp:80-83) as they stand after
+ * a full step: out = 8 host arrays (NX*NY*NZ; any may be NULL) receiving UU VV WW FU FV FW FR FT
+ * of the third stage's input state.  UU = RU * (1/RO) etc. over the whole local array, ghosts
+ * included (src/fluxes.cpp:131-165); FU..FT as r3d_gpu_fluxes forms them (interior cells; on the
+ * domain's top and bottom planes the momentum and energy entries are 0, where the reference keeps
+ * right-hand sides that BCON then overrides).  R3D_ESTATE unless the last operation on the state
+ * was a full 3-stage step; FP64 only; FU..FT are refused with density diffusion (ID).  The state
+ * is unchanged. */
+int r3d_gpu_download_work(r3d_gpu* g, double* const* out);
+
 /* Test hook for the failure path: from the next step on, every TMA transaction of the stage
  * kernels expects `bytes` more than its copies deliver, so each bounded wait runs out (200 ms),
  * the kernel records the error and returns, and the step reports R3D_ECUDA; the context stays

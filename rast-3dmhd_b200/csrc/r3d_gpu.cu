@@ -488,6 +488,7 @@ void enqueue_step(r3d_gpu* g, int nstages, Timer& tm, int& launches, int& stage_
         ++launches;
     }
     tm.end(2);
+    g->work_ok = nstages == 3;
 }
 
 void* state_field(r3d_gpu* g, int q, size_t* esize) {
@@ -582,6 +583,7 @@ void run_steps(r3d_gpu* g, int nsteps, r3d_scalars* sc, r3d_timing* tmout, bool 
         ++g->steps_enqueued;
         if (g->p.tc != 0.0 && n + 1 < nsteps) pull_scalars(g, nullptr);  // host clock for BCON
     }
+    if (nsteps > 0) g->work_ok = true;
     if (sync || tmout) pull_scalars(g, sc);
     if (tmout) {
         std::memset(tmout, 0, sizeof(*tmout));
@@ -1051,6 +1053,7 @@ void finish_state(r3d_gpu* g, const r3d_scalars* sc) {
     launch_dt_full_any(g);
     cuda_ok(cudaStreamSynchronize(g->stream), "upload");
     g->uploaded = true;
+    g->work_ok = false;
 }
 
 }  // namespace r3dg
@@ -1208,6 +1211,49 @@ int r3d_gpu_download_accumulators(r3d_gpu* g, double* const* z) {
     });
 }
 
+namespace r3dg {
+
+// FLUXES of the FP64 state in buffer set `buf` (without changing it) into host arrays out[0 ..
+// nfields-1] (NX*NY*NZ each, interior cells, ghosts 0); null entries are skipped.  The stage
+// kernel runs as a first stage with its F stored, into scratch kept by the handle.
+void eval_fluxes(r3d_gpu* g, int buf, double* const* out) {
+    const Derived& d = g->d;
+    const size_t fe = (size_t)g->geo.plane * d.nz;
+    const int nf = g->nfields;
+    if (!g->fscr) {
+        cuda_ok(cudaMalloc(&g->fscr, 3 * (size_t)nf * fe * sizeof(double)), "cudaMalloc(flux scratch)");
+        cuda_ok(cudaMemsetAsync(g->fscr, 0, 3 * (size_t)nf * fe * sizeof(double), g->stream), "cudaMemset");
+        g->bytes += (int64_t)(3 * (size_t)nf * fe * sizeof(double));
+    }
+    FieldSet fs{};
+    for (int q = 0; q < nf; ++q) {
+        fs.xin[q] = g->X[buf][q];
+        fs.xout[q] = g->fscr + (size_t)q * fe;                 // stage result, discarded
+        fs.z[q] = g->fscr + (size_t)(nf + q) * fe;             // accumulator, discarded
+        fs.f[q] = g->fscr + (size_t)(2 * nf + q) * fe;         // F
+    }
+    cuda_ok(r3dk::launch_stage_fp64(0, g->maps[buf], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk, g->stream,
+                                    true),
+            "fluxes");
+    std::vector<double> hb((size_t)(d.nx * d.ny * d.nz));
+    for (int q = 0; q < nf; ++q) {
+        if (!out[q]) continue;
+        cuda_ok(cudaMemcpy2DAsync(hb.data(), d.nx * sizeof(double), fs.f[q], g->geo.pitch * sizeof(double),
+                                  d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyDeviceToHost, g->stream),
+                "fluxes download");
+        cuda_ok(cudaStreamSynchronize(g->stream), "fluxes");
+        for (int64_t k = 0; k < d.nz; ++k)
+            for (int64_t j = 0; j < d.ny; ++j)
+                for (int64_t i = 0; i < d.nx; ++i) {
+                    const bool inner = k >= 1 && k <= d.nz - 2 && j >= 1 && j <= d.ny - 2 && i >= 1 && i <= d.nx - 2;
+                    const size_t n = (size_t)((k * d.ny + j) * d.nx + i);
+                    out[q][n] = inner ? hb[n] : 0.0;
+                }
+    }
+}
+
+}  // namespace r3dg
+
 int r3d_gpu_fluxes(r3d_gpu* g, double* const* out) {
     return guarded([&] {
         if (!g || !out) throw std::invalid_argument("null argument");
@@ -1215,40 +1261,47 @@ int r3d_gpu_fluxes(r3d_gpu* g, double* const* out) {
         if (g->fp32) throw Error(R3D_EINVAL, "r3d_gpu_fluxes needs precision fp64");
         if (g->p.id != 0) throw Error(R3D_EINVAL, "r3d_gpu_fluxes does not form the density diffusion (ID)");
         DeviceGuard dg(g->device);
-        const Derived& d = g->d;
-        const size_t fe = (size_t)g->geo.plane * d.nz;
-        const int nf = g->nfields;
-        if (!g->fscr) {
-            cuda_ok(cudaMalloc(&g->fscr, 3 * (size_t)nf * fe * sizeof(double)), "cudaMalloc(flux scratch)");
-            cuda_ok(cudaMemsetAsync(g->fscr, 0, 3 * (size_t)nf * fe * sizeof(double), g->stream), "cudaMemset");
-            g->bytes += (int64_t)(3 * (size_t)nf * fe * sizeof(double));
-        }
-        FieldSet fs{};
-        for (int q = 0; q < nf; ++q) {
-            fs.xin[q] = g->X[g->cur][q];
-            fs.xout[q] = g->fscr + (size_t)q * fe;                 // stage result, discarded
-            fs.z[q] = g->fscr + (size_t)(nf + q) * fe;             // accumulator, discarded
-            fs.f[q] = g->fscr + (size_t)(2 * nf + q) * fe;         // F
-        }
-        cuda_ok(r3dk::launch_stage_fp64(0, g->maps[g->cur], g->geo, g->ph, g->lines, fs, g->dsc, g->kchunk,
-                                        g->stream, true),
-                "fluxes");
-        std::vector<double> buf((size_t)(d.nx * d.ny * d.nz));
-        for (int q = 0; q < nf; ++q) {
+        for (int q = 0; q < g->nfields; ++q)
             if (!out[q]) throw std::invalid_argument("null output field");
-            cuda_ok(cudaMemcpy2DAsync(buf.data(), d.nx * sizeof(double), fs.f[q], g->geo.pitch * sizeof(double),
-                                      d.nx * sizeof(double), d.ny * d.nz, cudaMemcpyDeviceToHost, g->stream),
-                    "fluxes download");
-            cuda_ok(cudaStreamSynchronize(g->stream), "fluxes");
-            for (int64_t k = 0; k < d.nz; ++k)
-                for (int64_t j = 0; j < d.ny; ++j)
-                    for (int64_t i = 0; i < d.nx; ++i) {
-                        const bool inner = k >= 1 && k <= d.nz - 2 && j >= 1 && j <= d.ny - 2 && i >= 1 && i <= d.nx - 2;
-                        const size_t n = (size_t)((k * d.ny + j) * d.nx + i);
-                        out[q][n] = inner ? buf[n] : 0.0;
-                    }
-        }
+        eval_fluxes(g, g->cur, out);
         pull_scalars(g, nullptr);
+    });
+}
+
+int r3d_gpu_download_work(r3d_gpu* g, double* const* out) {
+    return guarded([&] {
+        if (!g || !out) throw std::invalid_argument("null argument");
+        if (!g->uploaded) throw Error(R3D_ESTATE, "download before upload");
+        if (g->fp32) throw Error(R3D_EINVAL, "r3d_gpu_download_work needs precision fp64");
+        if (!g->work_ok) throw Error(R3D_ESTATE, "no full step since the state was set");
+        bool want_f = false;
+        for (int q = 3; q < 8; ++q) want_f = want_f || out[q];
+        if (want_f && g->p.id != 0)
+            throw Error(R3D_EINVAL, "the fluxes with density diffusion (ID) are not formed outside a stage");
+        DeviceGuard dg(g->device);
+        const Derived& d = g->d;
+        const int prev = 1 - g->cur;  // after a full step: the third stage's input
+        const size_t cnt = (size_t)(d.nx * d.ny * d.nz);
+        if (out[0] || out[1] || out[2]) {
+            // UU = RU * (1/RO) etc. over the whole local array (src/fluxes.cpp:131-165)
+            std::vector<double> h(4 * cnt);
+            for (int q = 0; q < 4; ++q)
+                cuda_ok(cudaMemcpy2DAsync(h.data() + q * cnt, d.nx * sizeof(double), g->X[prev][q],
+                                          g->geo.pitch * sizeof(double), d.nx * sizeof(double), d.ny * d.nz,
+                                          cudaMemcpyDeviceToHost, g->stream),
+                        "download work");
+            cuda_ok(cudaStreamSynchronize(g->stream), "download work");
+            for (size_t n = 0; n < cnt; ++n) {
+                const double rinv = 1.0 / h[3 * cnt + n];
+                for (int q = 0; q < 3; ++q)
+                    if (out[q]) out[q][n] = h[q * cnt + n] * rinv;
+            }
+        }
+        if (want_f) {
+            double* fo[r3dk::kMaxFields] = {};
+            for (int q = 0; q < 5; ++q) fo[q] = out[3 + q];
+            eval_fluxes(g, prev, fo);
+        }
     });
 }
 

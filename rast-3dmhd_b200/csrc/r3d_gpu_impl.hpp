@@ -48,6 +48,7 @@ struct r3d_gpu {
     int cur = 0;
     int kchunk = 32;
     bool uploaded = false;
+    bool work_ok = false;  // the last operation on the state was a full step (r3d_gpu_download_work)
     int64_t bytes = 0;
     double host_timc = 0.0, host_timi = 0.0;  // host clock for the plume relaxation (tc != 0)
     std::vector<cudaEvent_t> ev;             // timing events (r3d_gpu_run_timed)

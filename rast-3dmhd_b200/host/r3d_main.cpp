@@ -93,10 +93,12 @@ double initial_dt(const r3d_params& p, const HostState& s) {
 
 // gstate dump, src/main.cpp:42-93: magic, counts, 13-int header, 27 scalars, 27 3D arrays and
 // 14 1D arrays each preceded by its int64 length, int64 -1.  The RK accumulators zru..ztt and
-// zbx..zbz are the device's (r3d_gpu_download_accumulators, interior cells).  The other work
-// arrays of the reference's dump (uu vv ww, fu..ft, ww1..ww3: temporaries of its FLUXES sweeps)
-// do not exist in the fused kernels and are written as zeros.
-void write_gstate(const r3d_params& p, const HostState& s, const r3d_scalars& sc, const char* tag, int iter) {
+// zbx..zbz are the device's (r3d_gpu_download_accumulators, interior cells).  `work` (after a
+// step; null at the start) holds uu vv ww fu fv fw fr ft of the last step's third-stage input
+// (r3d_gpu_download_work); the scratch arrays ww1..ww3, whose contents in the reference are
+// whatever its last FLUXES sweep left, are written as zeros, and so is anything work lacks.
+void write_gstate(const r3d_params& p, const HostState& s, const r3d_scalars& sc, const char* tag, int iter,
+                  const std::vector<std::vector<double>>* work = nullptr) {
     char fname[256];
     std::snprintf(fname, sizeof fname, "gstate.%s.%03d.%04d", tag, 0, iter);
     FILE* fp = std::fopen(fname, "wb");
@@ -120,15 +122,19 @@ void write_gstate(const r3d_params& p, const HostState& s, const r3d_scalars& sc
     w(scal, sizeof scal);
     // the reference's field order: ru rv rw ro tt uu vv ww fu fv fw fr ft zru zrv zrw zro ztt
     // ww1 ww2 ww3 bx by bz zbx zby zbz
-    // (primaries 0-7, accumulators 8-15, -1: not kept)
-    const int order[27] = {0, 1, 2, 3, 4, -1, -1, -1, -1, -1, -1, -1, -1, 8,
+    // (primaries 0-7, accumulators 8-15, work arrays 16-23, -1: not kept)
+    const int order[27] = {0, 1, 2, 3, 4, 16, 17, 18, 19, 20, 21, 22, 23, 8,
                            9, 10, 11, 12, -1, -1, -1, 5, 6, 7, 13, 14, 15};
     const int64_t cnt = s.nx * s.ny * s.nz;
     std::vector<double> zeros((size_t)cnt, 0.0);
     for (int q = 0; q < 27; ++q) {
         w(&cnt, 8);
         const int o = order[q];
-        w(o < 0 ? zeros.data() : (o < 8 ? s.f[o].data() : s.z[o - 8].data()), (size_t)cnt * 8);
+        const double* src = zeros.data();
+        if (o >= 0 && o < 8) src = s.f[o].data();
+        else if (o >= 8 && o < 16) src = s.z[o - 8].data();
+        else if (o >= 16 && work && !(*work)[o - 16].empty()) src = (*work)[o - 16].data();
+        w(src, (size_t)cnt * 8);
     }
     for (int q = 0; q < 14; ++q) {
         const int64_t c = (int64_t)s.line[q].size();
@@ -257,7 +263,19 @@ int main(int argc, char** argv) {
                 double* zp[8];
                 for (int q = 0; q < 8; ++q) zp[q] = s.z[q].data();
                 check(r3d_gpu_download_accumulators(g, zp), "r3d_gpu_download_accumulators");
-                write_gstate(p, s, sc, "step", sc.nit);
+                // FP64: uu vv ww and, without density diffusion, fu..ft of the step's third stage
+                std::vector<std::vector<double>> work(8);
+                if (p.precision == R3D_PREC_FP64) {
+                    double* wp[8] = {};
+                    const size_t cnt = (size_t)(s.nx * s.ny * s.nz);
+                    for (int q = 0; q < 8; ++q) {
+                        if (q >= 3 && p.id != 0) continue;
+                        work[q].assign(cnt, 0.0);
+                        wp[q] = work[q].data();
+                    }
+                    check(r3d_gpu_download_work(g, wp), "r3d_gpu_download_work");
+                }
+                write_gstate(p, s, sc, "step", sc.nit, &work);
             }
             const double wall = wall_since();
             std::fprintf(stderr, "NIT %d  DT %g  TIMC %g  UMACH %g  WALL %.1fs (%.2fs/step)\n", sc.nit, sc.dt, sc.timc,

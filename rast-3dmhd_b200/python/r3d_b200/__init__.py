@@ -115,6 +115,7 @@ def lib():
         L.r3d_gpu_debug_tma_extra.argtypes = [vp, ctypes.c_uint]
         L.r3d_gpu_debug_dt_filter.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         L.r3d_gpu_fluxes.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
+        L.r3d_gpu_download_work.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_double))]
         L.r3d_setup_host_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(_HostStateC),
                                           ctypes.POINTER(Scalars)]
         L.r3d_gpu_create_slab.argtypes = [ctypes.POINTER(Params), ip, ip, ctypes.POINTER(vp)]
@@ -374,6 +375,19 @@ class GpuSim:
         dp = ctypes.POINTER(ctypes.c_double)
         arr = (dp * len(names))(*[out[n].ctypes.data_as(dp) for n in names])
         _check(lib().r3d_gpu_fluxes(self.h, arr))
+        return out
+
+    def work(self, fluxes: bool = True) -> Dict[str, np.ndarray]:
+        """The FLUXES work arrays of a gstate dump after a full step: uu vv ww of the third stage's
+        input (+ fu fv fw fr ft unless fluxes=False), shapes (NZ, NY, NX)."""
+        NX, NY, NZ = dims(self.p)
+        if self.slab is not None:
+            NZ = self.slab[1] + 2
+        names = ["uu", "vv", "ww", "fu", "fv", "fw", "fr", "ft"]
+        out = {n: np.zeros((NZ, NY, NX)) for n in names[:8 if fluxes else 3]}
+        dp = ctypes.POINTER(ctypes.c_double)
+        arr = (dp * 8)(*[out[n].ctypes.data_as(dp) if n in out else dp() for n in names])
+        _check(lib().r3d_gpu_download_work(self.h, arr))
         return out
 
     def debug_tma_extra(self, nbytes: int):

@@ -74,6 +74,18 @@ def test_cli_run_dumps_match_oracle(tmp_path):
     for n in ("zru", "zrv", "zrw", "zro", "ztt"):
         assert np.array_equal(g5.fields[n][strict], o.field(n)[strict]), n
     assert np.abs(g5.fields["zro"][strict]).max() > 0
+    # the FLUXES work arrays of the fifth step's third stage: the velocities on every cell, the
+    # right-hand sides on the interior (momentum and energy on the planes strictly inside; the
+    # fused kernel leaves them 0 on the top and bottom planes, which BCON overrides)
+    for n in ("uu", "vv", "ww"):
+        assert np.array_equal(g5.fields[n], o.field(n)), n
+    assert np.array_equal(interior(g5.fields["fr"]), interior(o.field("fr")))
+    for n in ("fu", "fv", "fw", "ft"):
+        assert np.array_equal(g5.fields[n][strict], o.field(n)[strict]), n
+        assert not g5.fields[n][1].any() and not g5.fields[n][-2].any(), n
+    assert np.abs(g5.fields["ft"][strict]).max() > 0 and np.abs(g5.fields["uu"]).max() > 0
+    for n in ("ww1", "ww2", "ww3"):
+        assert not g5.fields[n].any(), n
     # --dump-mode 0: progress lines only
     r = run(flags + ["--dump-mode", "0"], tmp_path / "..")
     assert r.returncode == 0 and sum(ln.startswith("NIT ") for ln in r.stderr.splitlines()) == 3

@@ -68,3 +68,56 @@ def test_fluxes_uniform_state():
     for n in ("fu", "fv", "fr", "ft"):
         assert not F[n][inner].any(), n
     assert np.all(F["fw"][inner] == 0.625 * 1.5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,flags,steps", [CASES[0], CASES[2]], ids=["hydro", "mhd"])
+def test_download_work_is_the_last_third_stage(name, flags, steps):
+    """r3d_gpu_download_work after `steps` full steps: uu vv ww of the third stage's input on
+    every cell and its right-hand sides (the oracle's arrays after the same steps, which keep
+    the last FLUXES call's); the state is unchanged and stepping on stays bit-exact."""
+    p = R.parse(flags + ["--seed", "6"])
+    st = R.HostState.setup(p)
+    o = Oracle(flags).init(6)
+    with R.GpuSim(p) as sim:
+        sim.upload(st)
+        with pytest.raises(R.R3dError) as e:
+            sim.work()
+        assert e.value.code == R.R3D_ESTATE  # no step yet
+        sim.run(steps)
+        W = sim.work()
+        W2 = sim.work()
+        for _ in range(steps):
+            o.step()
+        for n in ("uu", "vv", "ww"):
+            assert np.array_equal(W[n], o.field(n)), n
+        for n in ("fu", "fv", "fw", "fr", "ft"):
+            ks = slice(2, -2) if n != "fr" else slice(1, -1)
+            assert np.array_equal(W[n][ks, 1:-1, 1:-1], o.field(n)[ks, 1:-1, 1:-1]), n
+            assert np.array_equal(W[n], W2[n]), n
+        sim.step(3)
+        o.step()
+        after = st.copy()
+        sim.download(after)
+        for n in ("ru", "rv", "rw", "ro", "tt"):
+            assert np.array_equal(after.fields[n][1:-1, 1:-1, 1:-1], o.field(n)[1:-1, 1:-1, 1:-1]), n
+        sim.step(2)  # a partial step leaves no third stage
+        with pytest.raises(R.R3dError) as e:
+            sim.work()
+        assert e.value.code == R.R3D_ESTATE
+
+
+@pytest.mark.gpu
+def test_download_work_with_density_diffusion():
+    """With ID the velocities are available and the right-hand sides refused."""
+    p = R.parse(["--npx", "16", "--npy", "12", "--npz", "20", "--ngrid", "0", "--id", "1", "--dh", "0.5",
+                 "--seed", "4"])
+    st = R.HostState.setup(p)
+    with R.GpuSim(p) as sim:
+        sim.upload(st)
+        sim.run(2)
+        W = sim.work(fluxes=False)
+        assert sorted(W) == ["uu", "vv", "ww"] and np.abs(W["uu"]).max() > 0
+        with pytest.raises(R.R3dError) as e:
+            sim.work()
+        assert e.value.code == R.R3D_EINVAL
