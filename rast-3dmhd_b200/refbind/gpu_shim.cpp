@@ -26,6 +26,7 @@
 // does for every collective; step_gpu uses the comm it is given.
 #include <mpi.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -89,12 +90,14 @@ struct HostBlock {
     int nx = 0, ny = 0, nz = 0;
     std::vector<double> f[8];   // ru rv rw ro tt bx by bz
     std::vector<double> z[8];   // zru .. ztt, zbx zby zbz
+    std::vector<double> w[8];   // uu vv ww fu fv fw fr ft: the FLUXES work arrays after a full step
     std::vector<double> lx[4], ly[4], lz[6];  // exx dxxdx d2xxdx2 ddx | wyy .. ddy | zee .. ddz rkapa dkapa
     void resize(int x, int y, int zz) {
         nx = x; ny = y; nz = zz;
         const size_t n = (size_t)x * y * zz;
         for (auto& a : f) a.assign(n, 0.0);
         for (auto& a : z) a.assign(n, 0.0);
+        for (auto& a : w) a.assign(n, 0.0);
         for (auto& a : lx) a.assign(x, 0.0);
         for (auto& a : ly) a.assign(y, 0.0);
         for (auto& a : lz) a.assign(zz, 0.0);
@@ -180,12 +183,16 @@ void block_global(const Derived& d, int mypey, int mypez, HostBlock& blk, HostBl
                 double* gz = glob.f[q].data() + ((size_t)kg * NY + jg) * nx;
                 double* bz = blk.z[q].data() + ((size_t)kl * ny + jl) * nx;
                 double* gzz = glob.z[q].data() + ((size_t)kg * NY + jg) * nx;
+                double* bw = blk.w[q].data() + ((size_t)kl * ny + jl) * nx;
+                double* gw = glob.w[q].data() + ((size_t)kg * NY + jg) * nx;
                 if (gather) {
                     memcpy(gz, b, nx * sizeof(double));
                     memcpy(gzz, bz, nx * sizeof(double));
+                    memcpy(gw, bw, nx * sizeof(double));
                 } else {
                     memcpy(b, gz, nx * sizeof(double));
                     memcpy(bz, gzz, nx * sizeof(double));
+                    memcpy(bw, gw, nx * sizeof(double));
                 }
             }
         }
@@ -225,10 +232,38 @@ void from_state(const SimState& s, HostBlock& blk) {
 }
 
 void to_state(HostBlock& blk, SimState& s) {
+    Field* w[8] = {&s.uu, &s.vv, &s.ww, &s.fu, &s.fv, &s.fw, &s.fr, &s.ft};
     for (int q = 0; q < 8; ++q) {
         memcpy(field_of(s, q)->data(), blk.f[q].data(), blk.f[q].size() * sizeof(double));
         memcpy(zfield_of(s, q)->data(), blk.z[q].data(), blk.z[q].size() * sizeof(double));
+        memcpy(w[q]->data(), blk.w[q].data(), blk.w[q].size() * sizeof(double));
     }
+}
+
+// A rank's FLUXES forms FU..FT on its own interior only (src/fluxes.cpp:74-76); the values a
+// block cut from the global arrays carries on its halo cells are not the rank's.
+void clear_flux_halo(HostBlock& blk) {
+    const int nx = blk.nx, ny = blk.ny, nz = blk.nz;
+    for (int q = 3; q < 8; ++q)
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i)
+                    if (k == 0 || k == nz - 1 || j == 0 || j == ny - 1 || i == 0 || i == nx - 1)
+                        blk.w[q][((size_t)k * ny + j) * nx + i] = 0.0;
+}
+
+// The dump's FLUXES work arrays of the handle's last full step (r3d_gpu_download_work); zeros
+// when the state has not taken a full step since it was uploaded, and in the FP32-bulk form,
+// which keeps no FP64 work arrays.
+void fetch_work(r3d_gpu* h, HostBlock& blk) {
+    std::vector<double*> w(8);
+    for (int q = 0; q < 8; ++q) w[q] = blk.w[q].data();
+    const int rc = r3d_gpu_download_work(h, w.data());
+    if (rc == R3D_ESTATE || rc == R3D_EINVAL) {
+        for (auto& a : blk.w) std::fill(a.begin(), a.end(), 0.0);
+        return;
+    }
+    ok(rc, "r3d_gpu_download_work");
 }
 
 constexpr int kTagField = 7100;
@@ -237,17 +272,22 @@ constexpr int kTagField = 7100;
 void send_block(HostBlock& blk, int dest, bool with_z) {
     for (int q = 0; q < 8; ++q) {
         MPI_Send(blk.f[q].data(), (int)blk.f[q].size(), MPI_DOUBLE, dest, kTagField + q, MPI_COMM_WORLD);
-        if (with_z)
+        if (with_z) {
             MPI_Send(blk.z[q].data(), (int)blk.z[q].size(), MPI_DOUBLE, dest, kTagField + 8 + q, MPI_COMM_WORLD);
+            MPI_Send(blk.w[q].data(), (int)blk.w[q].size(), MPI_DOUBLE, dest, kTagField + 30 + q, MPI_COMM_WORLD);
+        }
     }
 }
 void recv_block(HostBlock& blk, int src, bool with_z, bool with_lines) {
     for (int q = 0; q < 8; ++q) {
         MPI_Recv(blk.f[q].data(), (int)blk.f[q].size(), MPI_DOUBLE, src, kTagField + q, MPI_COMM_WORLD,
                  MPI_STATUS_IGNORE);
-        if (with_z)
+        if (with_z) {
             MPI_Recv(blk.z[q].data(), (int)blk.z[q].size(), MPI_DOUBLE, src, kTagField + 8 + q, MPI_COMM_WORLD,
                      MPI_STATUS_IGNORE);
+            MPI_Recv(blk.w[q].data(), (int)blk.w[q].size(), MPI_DOUBLE, src, kTagField + 30 + q, MPI_COMM_WORLD,
+                     MPI_STATUS_IGNORE);
+        }
     }
     if (with_lines) {
         for (auto& a : blk.ly) MPI_Recv(a.data(), (int)a.size(), MPI_DOUBLE, src, kTagField + 20, MPI_COMM_WORLD, MPI_STATUS_IGNORE);
@@ -398,6 +438,7 @@ void gpu_download(SimState& s, GpuSim& g) {
             std::vector<double*> z(8, nullptr);
             for (int q = 0; q < 8; ++q) z[q] = b.staged.z[q].data();
             ok(r3d_gpu_download_accumulators(b.h, z.data()), "r3d_gpu_download_accumulators");
+            fetch_work(b.h, b.staged);
         }
         to_state(b.staged, s);
         scalars_to(b.sc, s);
@@ -410,6 +451,7 @@ void gpu_download(SimState& s, GpuSim& g) {
             std::vector<double*> z(8, nullptr);
             for (int q = 0; q < 8; ++q) z[q] = b.staged.z[q].data();
             ok(r3d_gpu_download_accumulators(b.h, z.data()), "r3d_gpu_download_accumulators");
+            fetch_work(b.h, b.staged);
         }
         for (int r = npe - 1; r >= 0; --r) {
             int py, pz;
@@ -417,6 +459,7 @@ void gpu_download(SimState& s, GpuSim& g) {
             HostBlock blk;
             blk.resize(d.nx, d.ny, d.nz);
             block_global(d, py, pz, blk, b.staged, false);
+            clear_flux_halo(blk);
             if (r == 0) to_state(blk, s);
             else send_block(blk, r, true);
         }

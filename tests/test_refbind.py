@@ -9,7 +9,9 @@ reference's own tests/gpu_equivalence_test.cpp:143-174 requires of its CUDA path
 interiors (x/y ghost images included), the scalars and the header, and the RK accumulators
 zru..ztt on the planes strictly inside the domain (on the top and bottom planes the reference
 keeps momentum and energy fluxes that BCON overwrites; the fused kernel does not form them, so
-only the accumulator values there - never the state - differ).
+only the accumulator values there - never the state - differ), and the FLUXES work arrays of
+the last third stage: uu vv ww on every cell, FR on each rank's interior and FU FV FW FT on its
+planes strictly inside.
 """
 import glob
 import os
@@ -93,6 +95,15 @@ def test_gpu_backend_dumps_equal_cpu_backend(name, flags, ranks, tmp_path):
                 a, b = c.fields[n][strict], g.fields[n][strict]
                 assert np.array_equal(a, b), f"{f} {n}: max |gpu - cpu| = {float(np.abs(a - b).max()):.3e}"
                 assert np.abs(a).max() > 0.0 or n == "zrw", (f, n)
+            # the FLUXES work arrays of the last third stage: velocities on every cell, the
+            # right-hand sides on each rank's interior (momentum and energy strictly inside)
+            for n in ("uu", "vv", "ww"):
+                a, b = c.fields[n], g.fields[n]
+                assert np.array_equal(a, b), f"{f} {n}: max |gpu - cpu| = {float(np.abs(a - b).max()):.3e}"
+            interior3 = (slice(1, -1), slice(1, -1), slice(1, -1))
+            for n, sl in (("fr", interior3), ("fu", strict), ("fv", strict), ("fw", strict), ("ft", strict)):
+                a, b = c.fields[n][sl], g.fields[n][sl]
+                assert np.array_equal(a, b), f"{f} {n}: max |gpu - cpu| = {float(np.abs(a - b).max()):.3e}"
         for n in gstate.LINES:
             assert np.array_equal(c.lines[n], g.lines[n]), (f, n)
 
